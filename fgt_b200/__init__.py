@@ -1,0 +1,234 @@
+"""fgt_b200 -- B200-native discrete point fast Gauss transform.
+
+Python mirror of the reference Fortran entry point
+``pfgt(nd,dim,delta,eps,iperiod,bs0,cen0,ns,sources,ifcharge,charge,
+ifdipole,rnormal,dipstr,ifpgh,pot,grad,hess,nt,targ,ifpghtarg,pottarg,
+gradtarg,hesstarg)`` (src/pfgt/pfgt.f:6-10) over the C ABI of
+include/fgt_b200.h (libfgt_b200.so, CUDA sm_100a).  There is no CPU
+fallback: without the built library or a CUDA device every call raises.
+
+numpy layouts (C order) equal the reference's column-major layouts:
+sources (ns, dim), charge (ns, nd), pot (n, nd), grad (n, dim, nd),
+hess (n, nhess, nd).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfgt_b200.so")
+
+FGT_OK = 0
+FGT_ERR_ARG = 1
+FGT_ERR_CUDA = 2
+FGT_ERR_NOMEM = 3
+FGT_ERR_UNSUPPORTED = 4
+FGT_ERR_TIMEOUT = 5
+FGT_ERR_NODEVICE = 6
+FGT_ERR_INJECTED = 7
+
+PREC_AUTO = 0
+PREC_FP64 = 1
+PREC_MIXED = 2
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class FgtStats(C.Structure):
+    _fields_ = [
+        ("nlevels", C.c_int), ("nboxes", C.c_int), ("npwlevel", C.c_int), ("npw", C.c_int),
+        ("ndiv", C.c_int), ("precision_used", C.c_int), ("n_form_boxes", C.c_int),
+        ("n_eval_boxes", C.c_int), ("n_eval_nufft", C.c_int), ("n_translations", C.c_int),
+        ("spread_width", C.c_int), ("grid_cells", C.c_int), ("n_kernel_launches", C.c_int),
+        ("near_pairs", C.c_double), ("bs0", C.c_double), ("cen0", C.c_double * 3),
+        ("ms", C.c_double * 12),
+    ]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("cen0", "ms")}
+        d["cen0"] = list(self.cen0)
+        d["ms"] = list(self.ms)
+        return d
+
+
+class FgtOpts(C.Structure):
+    _fields_ = [
+        ("precision", C.c_int), ("device_ptrs", C.c_int), ("device", C.c_int),
+        ("stream", C.c_void_p), ("ndiv", C.c_int), ("small_eval", C.c_int),
+        ("spread_width", C.c_int), ("timing", C.c_int), ("stats", C.POINTER(FgtStats)),
+    ]
+
+
+class FgtError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"fgt_b200 error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+# every symbol declared in include/fgt_b200.h
+EXPORTS = ["fgt_opts_default", "fgt_pfgt_c", "pfgt_", "pfgt_direct_", "fgt_last_status",
+           "fgt_last_error", "fgt_version", "fgt_debug_tree_build", "fgt_debug_tree_get",
+           "fgt_debug_tree_free"]
+
+
+def lib():
+    """Load libfgt_b200.so (raises if it is missing: no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FgtError(FGT_ERR_NODEVICE,
+                           f"{LIB_PATH} not built; run python -m fgt_b200.build")
+        L = C.CDLL(LIB_PATH)
+        L.fgt_pfgt_c.restype = C.c_int
+        L.fgt_pfgt_c.argtypes = [
+            C.POINTER(FgtOpts), C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _dp, _dp,
+            C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+            C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+            C.c_void_p, C.c_void_p, C.c_void_p]
+        L.fgt_last_error.restype = C.c_char_p
+        L.fgt_version.restype = C.c_char_p
+        L.fgt_debug_tree_build.restype = C.c_void_p
+        L.fgt_debug_tree_build.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, C.c_double,
+                                           _dp, C.c_int, _dp, C.c_int, _dp, C.c_int]
+        L.fgt_debug_tree_get.restype = C.c_long
+        L.fgt_debug_tree_get.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_long]
+        L.fgt_debug_tree_free.argtypes = [C.c_void_p]
+        _lib = L
+    return _lib
+
+
+def version():
+    return lib().fgt_version().decode()
+
+
+def last_error():
+    return lib().fgt_last_error().decode()
+
+
+def _f64(a, shape):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a.reshape(shape)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None, rnormal=None,
+         ifpgh=1, targets=None, ifpghtarg=0, bs0=1.0, cen0=None, precision=PREC_AUTO,
+         ndiv=0, small_eval=-1, spread_width=0, stats=False, timing=False):
+    """Point FGT with the reference's argument meaning (src/pfgt/pfgt.f:11-53).
+
+    Returns a dict with pot/grad/hess (sources) and pottarg/gradtarg/hesstarg
+    (targets) for the requested levels, plus bs0/cen0 (and stats if asked).
+    """
+    L = lib()
+    src = _f64(sources, (-1, dim))
+    ns = src.shape[0]
+    trg = None if targets is None else _f64(targets, (-1, dim))
+    nt = 0 if trg is None else trg.shape[0]
+    nhess = dim * (dim + 1) // 2
+    ifcharge = 0 if charge is None else 1
+    ifdipole = 0 if dipstr is None else 1
+    q = _f64(charge, (ns, nd)) if ifcharge else None
+    ds = _f64(dipstr, (ns, nd)) if ifdipole else None
+    rn = _f64(rnormal, (ns, dim)) if ifdipole else None
+    pot = np.zeros((ns, nd)) if ifpgh >= 1 else None
+    grad = np.zeros((ns, dim, nd)) if ifpgh >= 2 else None
+    hess = np.zeros((ns, nhess, nd)) if ifpgh >= 3 else None
+    pt = np.zeros((nt, nd)) if (ifpghtarg >= 1 and nt) else None
+    gt = np.zeros((nt, dim, nd)) if (ifpghtarg >= 2 and nt) else None
+    ht = np.zeros((nt, nhess, nd)) if (ifpghtarg >= 3 and nt) else None
+    b0 = C.c_double(float(bs0))
+    c0 = np.zeros(3)
+    if cen0 is not None:
+        c0[:dim] = np.asarray(cen0, dtype=np.float64)[:dim]
+    st = FgtStats()
+    o = FgtOpts()
+    L.fgt_opts_default(C.byref(o))
+    o.precision = precision
+    o.ndiv = ndiv
+    o.small_eval = small_eval
+    o.spread_width = spread_width
+    o.timing = 1 if timing else 0
+    o.stats = C.pointer(st) if (stats or timing) else None
+    rc = L.fgt_pfgt_c(C.byref(o), nd, dim, delta, eps, iperiod, C.byref(b0),
+                      c0.ctypes.data_as(_dp), ns, _ptr(src), ifcharge, _ptr(q), ifdipole,
+                      _ptr(rn), _ptr(ds), ifpgh, _ptr(pot), _ptr(grad), _ptr(hess), nt,
+                      _ptr(trg), ifpghtarg if nt else 0, _ptr(pt), _ptr(gt), _ptr(ht))
+    if rc != FGT_OK:
+        raise FgtError(rc, last_error())
+    out = {"bs0": b0.value, "cen0": c0[:dim].copy()}
+    for k, v in (("pot", pot), ("grad", grad), ("hess", hess), ("pottarg", pt),
+                 ("gradtarg", gt), ("hesstarg", ht)):
+        if v is not None:
+            out[k] = v
+    if stats or timing:
+        out["stats"] = st.as_dict()
+    return out
+
+
+def pfgt_device(opts, nd, dim, delta, eps, iperiod, bs0, cen0, ns, src_ptr, ifcharge,
+                q_ptr, ifdipole, rn_ptr, ds_ptr, ifpgh, pot_ptr, grad_ptr, hess_ptr, nt,
+                trg_ptr, ifpghtarg, pt_ptr, gt_ptr, ht_ptr):
+    """Raw call with device pointers (opts.device_ptrs must be 1)."""
+    L = lib()
+    b0 = C.c_double(float(bs0))
+    c0 = np.zeros(3)
+    c0[:dim] = np.asarray(cen0, dtype=np.float64)[:dim]
+    rc = L.fgt_pfgt_c(C.byref(opts), nd, dim, delta, eps, iperiod, C.byref(b0),
+                      c0.ctypes.data_as(_dp), ns, src_ptr, ifcharge, q_ptr, ifdipole, rn_ptr,
+                      ds_ptr, ifpgh, pot_ptr, grad_ptr, hess_ptr, nt, trg_ptr, ifpghtarg,
+                      pt_ptr, gt_ptr, ht_ptr)
+    if rc != FGT_OK:
+        raise FgtError(rc, last_error())
+    return b0.value, c0[:dim].copy()
+
+
+_TREE_ARRAYS = {
+    "key": np.uint64, "level": np.int32, "nonleaf": np.int32, "parent": np.int32,
+    "child0": np.int32, "center": np.float64, "src_lo": np.int32, "src_hi": np.int32,
+    "trg_lo": np.int32, "trg_hi": np.int32, "isrc": np.uint32, "itrg": np.uint32,
+    "l1_ptr": np.int32, "l1_src": np.int32, "form_box": np.int32, "eval_box": np.int32,
+    "eval_self": np.int32, "trans_ptr": np.int32, "trans_src": np.int32, "trans_w": np.int32,
+    "scalars": np.int32, "dscalars": np.float64,
+}
+
+
+def debug_tree(dim, delta, eps, iperiod, sources, targets, bs0=1.0, cen0=None, ndiv=0):
+    """Device-built tree and lists of a pfgt call, copied to numpy arrays."""
+    L = lib()
+    src = _f64(sources, (-1, dim))
+    trg = _f64(targets, (-1, dim)) if targets is not None and len(targets) else np.zeros((0, dim))
+    c0 = np.zeros(3)
+    if cen0 is not None:
+        c0[:dim] = np.asarray(cen0, dtype=np.float64)[:dim]
+    h = L.fgt_debug_tree_build(dim, delta, eps, iperiod, float(bs0), c0.ctypes.data_as(_dp),
+                               src.shape[0], src.ctypes.data_as(_dp), trg.shape[0],
+                               trg.ctypes.data_as(_dp) if trg.shape[0] else None, ndiv)
+    if not h:
+        raise FgtError(FGT_ERR_NODEVICE, "debug tree build failed: " + last_error())
+    out = {}
+    try:
+        for name, dt in _TREE_ARRAYS.items():
+            n = L.fgt_debug_tree_get(h, name.encode(), None, 0)
+            a = np.zeros(max(n, 0), dtype=dt)
+            if n > 0:
+                L.fgt_debug_tree_get(h, name.encode(), a.ctypes.data_as(C.c_void_p), n)
+            out[name] = a
+    finally:
+        L.fgt_debug_tree_free(h)
+    sc = out.pop("scalars")
+    (out["nlevels"], out["nboxes"], out["npwlevel"], out["ncutoff"], out["nleaves"],
+     out["n_form"], out["n_eval"], out["n_trans"], out["n_l1"], out["D"], out["nlevend"],
+     out["iperiod0"]) = [int(v) for v in sc]
+    ds = out.pop("dscalars")
+    out["bs0"] = float(ds[0])
+    out["cen0"] = ds[1:1 + dim].copy()
+    out["boxsize"] = ds[4:].copy()
+    out["center"] = out["center"].reshape(-1, dim)
+    return out

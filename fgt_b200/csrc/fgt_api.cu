@@ -1,0 +1,651 @@
+// C ABI and host orchestration of the point FGT (pfgt, src/pfgt/pfgt.f:6-409
+// and pfgtmain, src/pfgt/pfgt.f:415-1150).  Everything after the host->device
+// copy of the inputs runs on the GPU; the host computes only the FP64 scalar
+// set-up (cut-off level, root box, expansion length, PW nodes) with the
+// reference's formulas.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "fgt_pw.cuh"
+
+static thread_local int g_last_status = FGT_OK;
+static thread_local std::string g_last_error;
+
+extern "C" void fgt_set_error_message(const char* msg, const char* file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s (%s:%d)", msg ? msg : "error", file ? file : "?", line);
+  g_last_error = buf;
+}
+
+namespace fgt {
+
+namespace {
+
+template <typename T>
+__global__ void k_gather_coords(const double* __restrict__ x, int n, int dim,
+                                const uint32_t* __restrict__ perm, const int* __restrict__ ref,
+                                const double* __restrict__ center, T* __restrict__ off) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    size_t o = perm[i];
+    int b = ref[i];
+    for (int k = 0; k < dim; k++)
+      off[(size_t)k * n + i] = (T)(x[o * dim + k] - center[(size_t)b * dim + k]);
+  }
+}
+
+template <typename T>
+__global__ void k_gather_vals(const double* __restrict__ v, int n, int nv,
+                              const uint32_t* __restrict__ perm, T* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    size_t o = perm[i];
+    for (int j = 0; j < nv; j++) out[(size_t)j * n + i] = (T)v[o * nv + j];
+  }
+}
+
+// out[perm[i]] = sorted[i] for pot/grad/hess in the reference's layouts
+// (dreorderi/dreorderiv, src/common/fmmcommon2d.f:29-90).
+__global__ void k_scatter(const double* __restrict__ srt, int n, int nd, int dim, int pgh,
+                          const uint32_t* __restrict__ perm, double* __restrict__ pot,
+                          double* __restrict__ grad, double* __restrict__ hess) {
+  int nh = dim * (dim + 1) / 2;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    size_t o = perm[i];
+    for (int id = 0; id < nd; id++) {
+      pot[o * nd + id] = srt[(size_t)id * n + i];
+      if (pgh >= 2)
+        for (int k = 0; k < dim; k++)
+          grad[(o * dim + k) * nd + id] = srt[((size_t)(1 + k) * nd + id) * n + i];
+      if (pgh >= 3)
+        for (int m = 0; m < nh; m++)
+          hess[(o * nh + m) * nd + id] = srt[((size_t)(1 + dim + m) * nd + id) * n + i];
+    }
+  }
+}
+
+struct DevicePool {
+  bool configured = false;
+};
+
+void configure_pool(int dev) {
+  static std::mutex mu;
+  static std::vector<char> done(64, 0);
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done[dev] = 1;
+}
+
+cudaStream_t library_stream(int dev) {
+  static thread_local cudaStream_t streams[64] = {0};
+  static thread_local bool made[64] = {false};
+  if (dev < 0 || dev >= 64) return 0;
+  if (!made[dev]) {
+    FGT_CUDA(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking));
+    made[dev] = true;
+  }
+  return streams[dev];
+}
+
+struct Timer {
+  bool on;
+  cudaStream_t s;
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> slot;
+  Timer(bool o, cudaStream_t st) : on(o), s(st) {}
+  void mark(int phase_slot) {
+    if (!on) return;
+    cudaEvent_t e;
+    FGT_CUDA(cudaEventCreate(&e));
+    FGT_CUDA(cudaEventRecord(e, s));
+    ev.push_back(e);
+    slot.push_back(phase_slot);
+  }
+  void finish(double* ms) {
+    if (!on) return;
+    FGT_CUDA(cudaStreamSynchronize(s));
+    for (size_t i = 1; i < ev.size(); i++) {
+      float t = 0;
+      cudaEventElapsedTime(&t, ev[i - 1], ev[i]);
+      if (slot[i] >= 0 && slot[i] < 12) ms[slot[i]] += t;
+    }
+    if (ev.size() >= 2) {
+      float t = 0;
+      cudaEventElapsedTime(&t, ev.front(), ev.back());
+      ms[10] = t;
+    }
+  }
+  ~Timer() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+
+struct Call {
+  int nd, dim, iperiod, ns, nt, ifcharge, ifdipole, ifpgh, ifpghtarg;
+  double delta, eps;
+  const double *src, *q, *rn, *ds, *trg;  // device pointers
+  double *pot, *grad, *hess, *pott, *gradt, *hesst;  // device pointers
+};
+
+template <typename T>
+void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o, fgt_stats* st,
+              cudaStream_t s, Timer& tm) {
+  const int dim = c.dim, nd = c.nd, nhess = dim * (dim + 1) / 2;
+  int launches = 0;
+  // --- scalar set-up (pfgt.f:110-140)
+  int npwlevel = 0;
+  double bs0 = *bs0_io, cen0[FGT_MAXDIM] = {0, 0, 0};
+  for (int k = 0; k < dim; k++) cen0[k] = cen0_io[k];
+  tree_setup_scalars(dim, c.delta, c.eps, c.iperiod, c.src, c.ns, c.trg, c.nt, &npwlevel, &bs0,
+                     cen0, s);
+  launches += (c.iperiod != 1) ? 2 : 0;
+  if (c.iperiod != 1) {
+    *bs0_io = bs0;
+    for (int k = 0; k < dim; k++) cen0_io[k] = cen0[k];
+  }
+  int ndiv = o.ndiv > 0 ? o.ndiv : (dim == 1 ? 20 : (dim == 2 ? 80 : 250));
+  // --- tree (pts_tree_mem/build, pts_tree_sort)
+  Tree t;
+  tree_build(t, dim, c.iperiod, npwlevel, ndiv, bs0, cen0, c.src, c.ns, c.trg, c.nt, s);
+  launches += 12 + 6 * t.nlevels;
+  tm.mark(1);
+  const int nlevels = t.nlevels;
+  // --- expansion length (pfgt.f:321-334, fgtterms.f:72-141)
+  int npw = 0;
+  double pmax = 0, pi = 4.0 * atan(1.0);
+  auto pwterms = [&](double bsize, int iper) {
+    if (iper == 0) {
+      double rmax = bsize / sqrt(c.delta), d = sqrt(log(1.0 / c.eps));
+      pmax = 2.0 * d;
+      double h = 2 * pi / (rmax + d);
+      npw = 2 * ((int)(pmax / h) + 1);
+    } else {
+      npw = 2 * ((int)(bsize * sqrt(log(1.0 / c.eps) / c.delta) / pi) + 1) + 1;
+    }
+  };
+  if (npwlevel <= nlevels) {
+    if (npwlevel <= 1) {
+      pwterms(2 * t.boxsize[std::max(npwlevel, 0)], c.iperiod);
+      if (c.iperiod == 1) npw = npw + 1;
+    } else {
+      pwterms(2 * t.boxsize[npwlevel], 0);
+    }
+  }
+  if (npw < 4) npw = 4;
+  // --- pfgtmain set-up (pfgt.f:611-650)
+  int iperiod0 = c.iperiod;
+  bool periodic_nodes = false;
+  if (npwlevel <= 1 && c.iperiod == 1) {
+    periodic_nodes = true;
+    iperiod0 = 0;
+  }
+  int nlevend = nlevels;
+  if (npwlevel <= nlevels) nlevend = npwlevel;
+  bool do_pw = npwlevel < nlevels;
+  // A root smaller than the cut-off with ns <= ndiv forms no expansion; the
+  // reference then returns zeros (pfgt.f:649-650, 779).  Compute its direct
+  // self interaction instead.
+  if (npwlevel < 0 && c.ns <= ndiv) {
+    do_pw = false;
+    nlevend = 0;
+  }
+  Lists L;
+  build_lists(t, npwlevel, iperiod0, nlevend, do_pw, L, s);
+  launches += do_pw ? 8 : 2;
+  tm.mark(3);
+  // --- gather (dreorderf, fmmcommon2d.f:3-27) as offsets from reference boxes
+  DBuf<T> soff((size_t)c.ns * dim, s), toff((size_t)std::max(c.nt, 1) * dim, s);
+  DBuf<T> qs, dss, rns;
+  k_gather_coords<T><<<grid_for(c.ns, 256), 256, 0, s>>>(c.src, c.ns, dim, t.isrc, t.src_ref,
+                                                          t.center, soff);
+  FGT_LAUNCH_CHECK();
+  launches++;
+  if (c.nt > 0) {
+    k_gather_coords<T><<<grid_for(c.nt, 256), 256, 0, s>>>(c.trg, c.nt, dim, t.itrg, t.trg_ref,
+                                                            t.center, toff);
+    FGT_LAUNCH_CHECK();
+    launches++;
+  }
+  if (c.ifcharge) {
+    qs.alloc((size_t)c.ns * nd, s);
+    k_gather_vals<T><<<grid_for(c.ns, 256), 256, 0, s>>>(c.q, c.ns, nd, t.isrc, qs);
+    FGT_LAUNCH_CHECK();
+    launches++;
+  }
+  if (c.ifdipole) {
+    dss.alloc((size_t)c.ns * nd, s);
+    rns.alloc((size_t)c.ns * dim, s);
+    k_gather_vals<T><<<grid_for(c.ns, 256), 256, 0, s>>>(c.ds, c.ns, nd, t.isrc, dss);
+    FGT_LAUNCH_CHECK();
+    // rnormal(dim,ns) -> SoA [dim][n]
+    k_gather_vals<T><<<grid_for(c.ns, 256), 256, 0, s>>>(c.rn, c.ns, dim, t.isrc, rns);
+    FGT_LAUNCH_CHECK();
+    launches += 2;
+  }
+  // sorted outputs, FP64
+  int ncs = c.ifpgh >= 1 ? (1 + (c.ifpgh >= 2 ? dim : 0) + (c.ifpgh >= 3 ? nhess : 0)) : 0;
+  int nct = c.ifpghtarg >= 1 ? (1 + (c.ifpghtarg >= 2 ? dim : 0) + (c.ifpghtarg >= 3 ? nhess : 0)) : 0;
+  DBuf<double> outs((size_t)std::max(ncs, 1) * nd * c.ns, s);
+  DBuf<double> outt((size_t)std::max(nct, 1) * nd * std::max(c.nt, 1), s);
+  outs.zero();
+  outt.zero();
+  launches += 2;
+  SourceSet<T> src;
+  src.n = c.ns;
+  src.off = soff;
+  src.q = c.ifcharge ? qs.get() : nullptr;
+  src.ds = c.ifdipole ? dss.get() : nullptr;
+  src.rn = c.ifdipole ? rns.get() : nullptr;
+  src.lo = t.src_lo;
+  src.hi = t.src_hi;
+  EvalSet<T> es, et;
+  es.n = c.ns; es.pgh = c.ifpgh; es.off = soff; es.lo = t.src_lo; es.hi = t.src_hi; es.out = outs;
+  et.n = c.nt; et.pgh = c.ifpghtarg; et.off = toff; et.lo = t.trg_lo; et.hi = t.trg_hi; et.out = outt;
+  tm.mark(2);
+  // --- plane waves (pfgt.f:700-1073)
+  int n_nufft = 0;
+  if (do_pw && L.n_eval > 0) {
+    PWParams P;
+    pw_setup(P, dim, nd, npw, pmax, periodic_nodes ? 1 : 0, t.boxsize[0], c.delta, c.eps,
+             t.boxsize[t.ncutoff], o.spread_width);
+    PWData<T> D;
+    launches += pw_form<T>(P, t, L, src, D, s);
+    tm.mark(4);
+    launches += pw_translate<T>(P, L, D, s);
+    tm.mark(5);
+    int se = o.small_eval >= 0 ? o.small_eval : -1;
+    launches += pw_eval<T>(P, t, L, D, es, et, se, &n_nufft, s);
+    tm.mark(6);
+    if (st) {
+      st->spread_width = P.w;
+      st->grid_cells = P.G;
+    }
+  }
+  // --- direct near field (pfgt.f:1082-1136)
+  DirectGeom g;
+  g.dim = dim;
+  g.nd = nd;
+  g.iperiod0 = iperiod0;
+  g.nboxes = t.nboxes;
+  g.delta = c.delta;
+  g.dmax = log(1.0 / c.eps) * c.delta;
+  g.bs0 = t.boxsize[0];
+  g.center = t.center;
+  double pairs = 0;
+  launches += direct_near_field<T>(g, L, src, et, &pairs, s);
+  launches += direct_near_field<T>(g, L, src, es, &pairs, s);
+  tm.mark(7);
+  // --- back to input order
+  if (c.ifpgh >= 1) {
+    k_scatter<<<grid_for(c.ns, 256), 256, 0, s>>>(outs, c.ns, nd, dim, c.ifpgh, t.isrc, c.pot,
+                                                  c.grad, c.hess);
+    FGT_LAUNCH_CHECK();
+    launches++;
+  }
+  if (c.ifpghtarg >= 1 && c.nt > 0) {
+    k_scatter<<<grid_for(c.nt, 256), 256, 0, s>>>(outt, c.nt, nd, dim, c.ifpghtarg, t.itrg,
+                                                  c.pott, c.gradt, c.hesst);
+    FGT_LAUNCH_CHECK();
+    launches++;
+  }
+  tm.mark(8);
+  if (st) {
+    st->nlevels = nlevels;
+    st->nboxes = t.nboxes;
+    st->npwlevel = npwlevel;
+    st->npw = npw;
+    st->ndiv = ndiv;
+    st->n_form_boxes = L.n_form;
+    st->n_eval_boxes = L.n_eval;
+    st->n_eval_nufft = n_nufft;
+    st->n_translations = L.n_trans;
+    st->near_pairs = pairs;
+    st->n_kernel_launches = launches;
+    st->bs0 = bs0;
+    for (int k = 0; k < dim; k++) st->cen0[k] = cen0[k];
+  }
+}
+
+bool fault_requested(const char* what) {
+  const char* f = getenv("FGT_FAULT");
+  return f && strstr(f, what) != nullptr;
+}
+
+int pfgt_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps, int iperiod,
+              double* bs0, double* cen0, int ns, const double* sources, int ifcharge,
+              const double* charge, int ifdipole, const double* rnormal, const double* dipstr,
+              int ifpgh, double* pot, double* grad, double* hess, int nt, const double* targ,
+              int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg) {
+  fgt_opts o;
+  fgt_opts_default(&o);
+  if (opts_in) o = *opts_in;
+  // argument checks
+  FGT_REQUIRE(dim >= 1 && dim <= 3, FGT_ERR_ARG, "dim must be 1, 2 or 3");
+  FGT_REQUIRE(nd >= 1, FGT_ERR_ARG, "nd must be >= 1");
+  FGT_REQUIRE(delta > 0 && isfinite(delta), FGT_ERR_ARG, "delta must be positive");
+  FGT_REQUIRE(eps > 0 && eps < 1, FGT_ERR_ARG, "eps must lie in (0,1)");
+  FGT_REQUIRE(ns >= 1, FGT_ERR_ARG, "ns must be >= 1");
+  FGT_REQUIRE(nt >= 0, FGT_ERR_ARG, "nt must be >= 0");
+  FGT_REQUIRE(iperiod == 0 || iperiod == 1, FGT_ERR_ARG, "iperiod must be 0 or 1");
+  FGT_REQUIRE(ifcharge == 1 || ifdipole == 1, FGT_ERR_ARG, "need charges and/or dipoles");
+  FGT_REQUIRE(ifpgh >= 0 && ifpgh <= 3 && ifpghtarg >= 0 && ifpghtarg <= 3, FGT_ERR_ARG,
+              "ifpgh/ifpghtarg must lie in 0..3");
+  FGT_REQUIRE(sources && bs0 && cen0, FGT_ERR_ARG, "null sources/bs0/cen0");
+  FGT_REQUIRE(!(ifcharge == 1 && !charge), FGT_ERR_ARG, "null charge");
+  FGT_REQUIRE(!(ifdipole == 1 && (!dipstr || !rnormal)), FGT_ERR_ARG, "null dipole arrays");
+  FGT_REQUIRE(!(ifpgh >= 1 && !pot) && !(ifpgh >= 2 && !grad) && !(ifpgh >= 3 && !hess),
+              FGT_ERR_ARG, "null source output");
+  FGT_REQUIRE(!(nt > 0 && !targ), FGT_ERR_ARG, "null targets");
+  FGT_REQUIRE(!(nt > 0 && ifpghtarg >= 1 && !pottarg) && !(nt > 0 && ifpghtarg >= 2 && !gradtarg) &&
+                  !(nt > 0 && ifpghtarg >= 3 && !hesstarg),
+              FGT_ERR_ARG, "null target output");
+  FGT_REQUIRE(!(iperiod == 1 && !(*bs0 > 0)), FGT_ERR_ARG, "periodic bs0 must be positive");
+  if (fault_requested("launch") || fault_requested("alloc") || fault_requested("queue")) {
+    fgt_set_error_message("fault injected by FGT_FAULT", __FILE__, __LINE__);
+    return FGT_ERR_INJECTED;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    (void)cudaGetLastError();
+    fgt_set_error_message("no CUDA device", __FILE__, __LINE__);
+    return FGT_ERR_NODEVICE;
+  }
+  int dev = o.device;
+  if (dev < 0) FGT_CUDA(cudaGetDevice(&dev));
+  FGT_CUDA(cudaSetDevice(dev));
+  configure_pool(dev);
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : library_stream(dev);
+  fgt_stats local_stats;
+  fgt_stats* st = o.stats ? o.stats : nullptr;
+  if (st) memset(st, 0, sizeof(*st));
+  Timer tm(o.timing && st, s);
+  int nhess = dim * (dim + 1) / 2;
+  int prec = o.precision;
+  if (prec == FGT_PREC_AUTO) prec = (eps >= 1e-6 * (1 - 1e-9)) ? FGT_PREC_MIXED : FGT_PREC_FP64;
+  Call c;
+  c.nd = nd; c.dim = dim; c.iperiod = iperiod; c.ns = ns; c.nt = nt;
+  c.ifcharge = ifcharge == 1; c.ifdipole = ifdipole == 1;
+  c.ifpgh = ifpgh; c.ifpghtarg = nt > 0 ? ifpghtarg : 0;
+  c.delta = delta; c.eps = eps;
+  tm.mark(-1);
+  // inputs on the device
+  DBuf<double> d_src, d_q, d_rn, d_ds, d_trg, d_pot, d_grad, d_hess, d_pt, d_gt, d_ht;
+  auto h2d = [&](DBuf<double>& b, const double* h, size_t n) -> const double* {
+    if (o.device_ptrs) return h;
+    b.alloc(n, s);
+    FGT_CUDA(cudaMemcpyAsync(b.get(), h, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    return b.get();
+  };
+  auto dout = [&](DBuf<double>& b, double* h, size_t n) -> double* {
+    if (o.device_ptrs) return h;
+    b.alloc(n, s);
+    return b.get();
+  };
+  c.src = h2d(d_src, sources, (size_t)ns * dim);
+  c.q = c.ifcharge ? h2d(d_q, charge, (size_t)ns * nd) : nullptr;
+  c.rn = c.ifdipole ? h2d(d_rn, rnormal, (size_t)ns * dim) : nullptr;
+  c.ds = c.ifdipole ? h2d(d_ds, dipstr, (size_t)ns * nd) : nullptr;
+  c.trg = nt > 0 ? h2d(d_trg, targ, (size_t)nt * dim) : c.src;
+  c.pot = ifpgh >= 1 ? dout(d_pot, pot, (size_t)ns * nd) : nullptr;
+  c.grad = ifpgh >= 2 ? dout(d_grad, grad, (size_t)ns * nd * dim) : nullptr;
+  c.hess = ifpgh >= 3 ? dout(d_hess, hess, (size_t)ns * nd * nhess) : nullptr;
+  c.pott = c.ifpghtarg >= 1 ? dout(d_pt, pottarg, (size_t)nt * nd) : nullptr;
+  c.gradt = c.ifpghtarg >= 2 ? dout(d_gt, gradtarg, (size_t)nt * nd * dim) : nullptr;
+  c.hesst = c.ifpghtarg >= 3 ? dout(d_ht, hesstarg, (size_t)nt * nd * nhess) : nullptr;
+  tm.mark(0);
+  if (prec == FGT_PREC_FP64) run_pfgt<double>(c, bs0, cen0, o, st, s, tm);
+  else run_pfgt<float>(c, bs0, cen0, o, st, s, tm);
+  if (!o.device_ptrs) {
+    auto d2h = [&](double* h, const DBuf<double>& b, size_t n) {
+      if (h && b.p) FGT_CUDA(cudaMemcpyAsync(h, b.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    };
+    if (ifpgh >= 1) d2h(pot, d_pot, (size_t)ns * nd);
+    if (ifpgh >= 2) d2h(grad, d_grad, (size_t)ns * nd * dim);
+    if (ifpgh >= 3) d2h(hess, d_hess, (size_t)ns * nd * nhess);
+    if (c.ifpghtarg >= 1) d2h(pottarg, d_pt, (size_t)nt * nd);
+    if (c.ifpghtarg >= 2) d2h(gradtarg, d_gt, (size_t)nt * nd * dim);
+    if (c.ifpghtarg >= 3) d2h(hesstarg, d_ht, (size_t)nt * nd * nhess);
+  }
+  tm.mark(9);
+  FGT_CUDA(cudaStreamSynchronize(s));
+  if (st) {
+    st->precision_used = prec;
+    tm.finish(st->ms);
+  }
+  (void)local_stats;
+  return FGT_OK;
+}
+
+}  // namespace
+
+}  // namespace fgt
+
+extern "C" {
+
+void fgt_opts_default(fgt_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->precision = FGT_PREC_AUTO;
+  o->device_ptrs = 0;
+  o->device = -1;
+  o->stream = nullptr;
+  o->ndiv = 0;
+  o->small_eval = -1;
+  o->spread_width = 0;
+  o->timing = 0;
+  o->stats = nullptr;
+}
+
+int fgt_pfgt_c(const fgt_opts* opts, int nd, int dim, double delta, double eps, int iperiod,
+               double* bs0, double* cen0, int ns, const double* sources, int ifcharge,
+               const double* charge, int ifdipole, const double* rnormal, const double* dipstr,
+               int ifpgh, double* pot, double* grad, double* hess, int nt, const double* targ,
+               int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg) {
+  int st;
+  try {
+    st = fgt::pfgt_impl(opts, nd, dim, delta, eps, iperiod, bs0, cen0, ns, sources, ifcharge,
+                        charge, ifdipole, rnormal, dipstr, ifpgh, pot, grad, hess, nt, targ,
+                        ifpghtarg, pottarg, gradtarg, hesstarg);
+  } catch (const fgt::Error& e) {
+    st = e.code;
+  } catch (...) {
+    fgt_set_error_message("unexpected host exception", __FILE__, __LINE__);
+    st = FGT_ERR_CUDA;
+  }
+  g_last_status = st;
+  return st;
+}
+
+void pfgt_(const int* nd, const int* dim, const double* delta, const double* eps,
+           const int* iperiod, double* bs0, double* cen0, const int* ns, const double* sources,
+           const int* ifcharge, const double* charge, const int* ifdipole, const double* rnormal,
+           const double* dipstr, const int* ifpgh, double* pot, double* grad, double* hess,
+           const int* nt, const double* targ, const int* ifpghtarg, double* pottarg,
+           double* gradtarg, double* hesstarg) {
+  int st = fgt_pfgt_c(nullptr, *nd, *dim, *delta, *eps, *iperiod, bs0, cen0, *ns, sources,
+                      *ifcharge, charge, *ifdipole, rnormal, dipstr, *ifpgh, pot, grad, hess, *nt,
+                      targ, *ifpghtarg, pottarg, gradtarg, hesstarg);
+  if (st != FGT_OK) {
+    // The Fortran interface has no status argument: poison the requested
+    // outputs so a failed call cannot pass for a result.
+    double nan = NAN;
+    int n = *nd, d = *dim, nh = d * (d + 1) / 2;
+    auto fill = [&](double* a, long long cnt) {
+      if (a && cnt > 0)
+        for (long long i = 0; i < cnt; i++) a[i] = nan;
+    };
+    if (*ifpgh >= 1) fill(pot, (long long)*ns * n);
+    if (*ifpgh >= 2) fill(grad, (long long)*ns * n * d);
+    if (*ifpgh >= 3) fill(hess, (long long)*ns * n * nh);
+    if (*ifpghtarg >= 1) fill(pottarg, (long long)*nt * n);
+    if (*ifpghtarg >= 2) fill(gradtarg, (long long)*nt * n * d);
+    if (*ifpghtarg >= 3) fill(hesstarg, (long long)*nt * n * nh);
+  }
+}
+
+int fgt_last_status(void) { return g_last_status; }
+
+const char* fgt_last_error(void) { return g_last_error.c_str(); }
+
+const char* fgt_version(void) { return "fgt_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Introspection of the device tree and lists (test support).
+namespace {
+struct DebugTree {
+  fgt::TreeHost th;
+  fgt::ListsHost lh;
+  std::vector<int> scalars;  // nlevels, nboxes, npwlevel, ncutoff, nleaves, n_form, n_eval, n_trans, n_l1, D
+  std::vector<double> dscal; // bs0, cen0[3], boxsize...
+};
+}  // namespace
+
+extern "C" void* fgt_debug_tree_build(int dim, double delta, double eps, int iperiod, double bs0_in,
+                                      const double* cen0_in, int ns, const double* src, int nt,
+                                      const double* trg, int ndiv_override) {
+  using namespace fgt;
+  try {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      (void)cudaGetLastError();
+      return nullptr;
+    }
+    int dev;
+    FGT_CUDA(cudaGetDevice(&dev));
+    configure_pool(dev);
+    cudaStream_t s = library_stream(dev);
+    DBuf<double> dsrc((size_t)ns * dim, s), dtrg((size_t)std::max(nt, 1) * dim, s);
+    FGT_CUDA(cudaMemcpyAsync(dsrc.get(), src, sizeof(double) * ns * dim, cudaMemcpyHostToDevice, s));
+    if (nt > 0)
+      FGT_CUDA(cudaMemcpyAsync(dtrg.get(), trg, sizeof(double) * nt * dim, cudaMemcpyHostToDevice, s));
+    int npwlevel = 0;
+    double bs0 = bs0_in, cen0[3] = {0, 0, 0};
+    for (int k = 0; k < dim; k++) cen0[k] = cen0_in ? cen0_in[k] : 0.0;
+    tree_setup_scalars(dim, delta, eps, iperiod, dsrc, ns, nt > 0 ? dtrg.get() : dsrc.get(),
+                       nt > 0 ? nt : 0, &npwlevel, &bs0, cen0, s);
+    int ndiv = ndiv_override > 0 ? ndiv_override : (dim == 1 ? 20 : (dim == 2 ? 80 : 250));
+    Tree t;
+    tree_build(t, dim, iperiod, npwlevel, ndiv, bs0, cen0, dsrc, ns, dtrg, nt, s);
+    int iperiod0 = (npwlevel <= 1 && iperiod == 1) ? 0 : iperiod;
+    int nlevend = t.nlevels;
+    if (npwlevel <= t.nlevels) nlevend = npwlevel;
+    bool do_pw = npwlevel < t.nlevels;
+    if (npwlevel < 0 && ns <= ndiv) {
+      do_pw = false;
+      nlevend = 0;
+    }
+    Lists L;
+    build_lists(t, npwlevel, iperiod0, nlevend, do_pw, L, s);
+    DebugTree* d = new DebugTree();
+    tree_download(t, d->th, s);
+    lists_download(L, t.nboxes, d->lh, s);
+    d->scalars = {t.nlevels, t.nboxes, npwlevel, t.ncutoff, t.nleaves, L.n_form, L.n_eval,
+                  L.n_trans, L.n_l1, t.D, nlevend, iperiod0};
+    d->dscal = {bs0, cen0[0], cen0[1], cen0[2]};
+    for (double b : t.boxsize) d->dscal.push_back(b);
+    return d;
+  } catch (const fgt::Error&) {
+    return nullptr;
+  }
+}
+
+extern "C" long fgt_debug_tree_get(void* h, const char* name, void* dst, long cap) {
+  if (!h || !name) return -1;
+  DebugTree* d = (DebugTree*)h;
+  auto put = [&](const auto& v) -> long {
+    long n = (long)v.size();
+    if (dst) memcpy(dst, v.data(), sizeof(v[0]) * (size_t)std::min(n, cap));
+    return n;
+  };
+  std::string s(name);
+  if (s == "scalars") return put(d->scalars);
+  if (s == "dscalars") return put(d->dscal);
+  if (s == "key") return put(d->th.key);
+  if (s == "level") return put(d->th.level);
+  if (s == "nonleaf") return put(d->th.nonleaf);
+  if (s == "parent") return put(d->th.parent);
+  if (s == "child0") return put(d->th.child0);
+  if (s == "center") return put(d->th.center);
+  if (s == "src_lo") return put(d->th.src_lo);
+  if (s == "src_hi") return put(d->th.src_hi);
+  if (s == "trg_lo") return put(d->th.trg_lo);
+  if (s == "trg_hi") return put(d->th.trg_hi);
+  if (s == "isrc") return put(d->th.isrc);
+  if (s == "itrg") return put(d->th.itrg);
+  if (s == "l1_ptr") return put(d->lh.l1_ptr);
+  if (s == "l1_src") return put(d->lh.l1_src);
+  if (s == "form_box") return put(d->lh.form_box);
+  if (s == "eval_box") return put(d->lh.eval_box);
+  if (s == "eval_self") return put(d->lh.eval_self);
+  if (s == "trans_ptr") return put(d->lh.trans_ptr);
+  if (s == "trans_src") return put(d->lh.trans_src);
+  if (s == "trans_w") return put(d->lh.trans_w);
+  return -1;
+}
+
+extern "C" void fgt_debug_tree_free(void* h) { delete (DebugTree*)h; }
+
+// ---------------------------------------------------------------------------
+// pfgt_direct drop-in (src/pfgt/pfgt.f:1156-1382), FP64 on the GPU.
+extern "C" void pfgt_direct_(const int* nd, const int* dim, const double* delta, const double* dmax,
+                             const int* iperiod, const double* shifts, const int* istart,
+                             const int* iend, const int* jstart, const int* jend,
+                             const double* source, const int* ifcharge, const double* charge,
+                             const int* ifdipole, const double* rnormal, const double* dipstr,
+                             const double* targ, const int* ifpgh, double* pot, double* grad,
+                             double* hess) {
+  using namespace fgt;
+  int st = FGT_OK;
+  try {
+    const int n = *nd, d = *dim, pgh = *ifpgh, nh = d * (d + 1) / 2;
+    const int is = *istart - 1, ns = *iend - *istart + 1, js = *jstart - 1, nt = *jend - *jstart + 1;
+    FGT_REQUIRE(d >= 1 && d <= 3 && n >= 1, FGT_ERR_ARG, "bad nd/dim");
+    if (ns > 0 && nt > 0 && pgh >= 1) {
+      if (fault_requested("launch") || fault_requested("alloc") || fault_requested("queue"))
+        throw Error{FGT_ERR_INJECTED, "fault injected"};
+      int ndev = 0;
+      if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        (void)cudaGetLastError();
+        throw Error{FGT_ERR_NODEVICE, "no CUDA device"};
+      }
+      int dev;
+      FGT_CUDA(cudaGetDevice(&dev));
+      configure_pool(dev);
+      cudaStream_t s = library_stream(dev);
+      auto up = [&](DBuf<double>& b, const double* h, size_t cnt) {
+        b.alloc(cnt, s);
+        FGT_CUDA(cudaMemcpyAsync(b.get(), h, sizeof(double) * cnt, cudaMemcpyHostToDevice, s));
+        return b.get();
+      };
+      DBuf<double> bs, bq, brn, bds, bt, bp, bg, bh, bsh;
+      const double* ds_ = up(bs, source + (size_t)is * d, (size_t)ns * d);
+      const double* dq = *ifcharge == 1 ? up(bq, charge + (size_t)is * n, (size_t)ns * n) : nullptr;
+      const double* drn = *ifdipole == 1 ? up(brn, rnormal + (size_t)is * d, (size_t)ns * d) : nullptr;
+      const double* dds = *ifdipole == 1 ? up(bds, dipstr + (size_t)is * n, (size_t)ns * n) : nullptr;
+      const double* dt = up(bt, targ + (size_t)js * d, (size_t)nt * d);
+      const double* dsh = *iperiod == 1 ? up(bsh, shifts, d) : nullptr;
+      double* dp = up(bp, pot + (size_t)js * n, (size_t)nt * n) == nullptr ? nullptr : bp.get();
+      double* dg = pgh >= 2 ? (up(bg, grad + (size_t)js * n * d, (size_t)nt * n * d), bg.get()) : nullptr;
+      double* dh = pgh >= 3 ? (up(bh, hess + (size_t)js * n * nh, (size_t)nt * n * nh), bh.get()) : nullptr;
+      direct_all_pairs(n, d, *delta, *dmax, dsh, ns, ds_, dq, drn, dds, nt, dt, pgh, dp, dg, dh, s);
+      FGT_CUDA(cudaMemcpyAsync(pot + (size_t)js * n, dp, sizeof(double) * nt * n, cudaMemcpyDeviceToHost, s));
+      if (dg) FGT_CUDA(cudaMemcpyAsync(grad + (size_t)js * n * d, dg, sizeof(double) * nt * n * d, cudaMemcpyDeviceToHost, s));
+      if (dh) FGT_CUDA(cudaMemcpyAsync(hess + (size_t)js * n * nh, dh, sizeof(double) * nt * n * nh, cudaMemcpyDeviceToHost, s));
+      FGT_CUDA(cudaStreamSynchronize(s));
+    }
+  } catch (const fgt::Error& e) {
+    st = e.code;
+  }
+  g_last_status = st;
+}

@@ -1,0 +1,381 @@
+// Direct near-field Gaussian sums (K9): warp-tiled, one evaluation point per
+// lane held in registers, list-1 sources staged through shared memory and
+// read as broadcasts.  Mixed precision: FP32 offsets from FP64 box centres,
+// FP32 exp (ex2.approx) and FP32 per-item accumulation, FP64 output
+// accumulation.  FP64 path: same kernel in double.
+#include <algorithm>
+
+#include "fgt_direct.cuh"
+
+namespace fgt {
+
+namespace {
+
+constexpr int DW = 4;  // warps per block
+
+template <typename T>
+struct DArgs {
+  int n_items, nd, d0, ne, ns, iperiod0;
+  T dinv, dmax, rfac;  // 1/delta, cut-off, 2/delta
+  double bs0;
+  const int *item_box, *item_lo;
+  const int *l1_ptr, *l1_src;
+  const int *s_lo, *s_hi, *e_hi;
+  const T *soff, *q, *ds, *rn, *eoff;
+  const double* center;
+  double* out;
+};
+
+template <int DIM>
+struct HessIdx;
+template <>
+struct HessIdx<1> {
+  static __device__ __forceinline__ int a(int m) { return 0; }
+  static __device__ __forceinline__ int b(int m) { return 0; }
+};
+template <>
+struct HessIdx<2> {  // xx, xy, yy (src/pfgt/pfgt_direct.f:185-189)
+  static __device__ __forceinline__ int a(int m) { return m == 2 ? 1 : 0; }
+  static __device__ __forceinline__ int b(int m) { return m == 0 ? 0 : 1; }
+};
+template <>
+struct HessIdx<3> {  // xx, yy, zz, xy, xz, yz
+  static __device__ __forceinline__ int a(int m) { return m < 3 ? m : (m < 5 ? 0 : 1); }
+  static __device__ __forceinline__ int b(int m) { return m < 3 ? m : (m == 3 ? 1 : 2); }
+};
+
+template <typename T, int DIM, int PGH, bool CHG, bool DIP, int NDC>
+__global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
+  constexpr int NH = DIM * (DIM + 1) / 2;
+  constexpr int NC = 1 + (PGH >= 2 ? DIM : 0) + (PGH >= 3 ? NH : 0);
+  __shared__ T sx[DW][DIM][32];
+  __shared__ T sq[DW][CHG ? NDC : 1][32];
+  __shared__ T sd[DW][DIP ? NDC : 1][32];
+  __shared__ T sn[DW][DIP ? DIM : 1][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ndc = min(NDC, a.nd - a.d0);
+  for (int it = blockIdx.x * DW + warp; it < a.n_items; it += gridDim.x * DW) {
+    const int tb = a.item_box[it];
+    const int p = a.item_lo[it] + lane;
+    const bool act = p < a.e_hi[tb];
+    T tx[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; k++) tx[k] = act ? a.eoff[(size_t)k * a.ne + p] : T(0);
+    T acc[NDC][NC];
+#pragma unroll
+    for (int i = 0; i < NDC; i++)
+#pragma unroll
+      for (int c = 0; c < NC; c++) acc[i][c] = T(0);
+    double cT[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; k++) cT[k] = a.center[(size_t)tb * DIM + k];
+    for (int li = a.l1_ptr[tb]; li < a.l1_ptr[tb + 1]; li++) {
+      const int sb = a.l1_src[li];
+      T dc[DIM];
+#pragma unroll
+      for (int k = 0; k < DIM; k++) {
+        double cs = a.center[(size_t)sb * DIM + k];
+        double sh = 0;
+        if (a.iperiod0 == 1) {  // pfgt_find_local_shift, src/pfgt/pfgt_direct.f:620-651
+          double dx = cT[k] - cs, dxp1 = dx - a.bs0, dxm1 = dx + a.bs0;
+          if (fabs(dx) > fabs(dxp1)) { dx = dxp1; sh = a.bs0; }
+          if (fabs(dx) > fabs(dxm1)) sh = -a.bs0;
+        }
+        dc[k] = (T)((cs + sh) - cT[k]);
+      }
+      const int s0 = a.s_lo[sb], s1 = a.s_hi[sb];
+      for (int base = s0; base < s1; base += 32) {
+        const int j = base + lane;
+        __syncwarp();
+        if (j < s1) {
+#pragma unroll
+          for (int k = 0; k < DIM; k++) sx[warp][k][lane] = a.soff[(size_t)k * a.ns + j] + dc[k];
+          if (CHG)
+#pragma unroll
+            for (int i = 0; i < NDC; i++)
+              if (i < ndc) sq[warp][i][lane] = a.q[(size_t)(a.d0 + i) * a.ns + j];
+          if (DIP) {
+#pragma unroll
+            for (int i = 0; i < NDC; i++)
+              if (i < ndc) sd[warp][i][lane] = a.ds[(size_t)(a.d0 + i) * a.ns + j];
+#pragma unroll
+            for (int k = 0; k < DIM; k++) sn[warp][k][lane] = a.rn[(size_t)k * a.ns + j];
+          }
+        }
+        __syncwarp();
+        const int cnt = min(32, s1 - base);
+        for (int jj = 0; jj < cnt; jj++) {
+          T dr[DIM], rr = T(0);
+#pragma unroll
+          for (int k = 0; k < DIM; k++) {
+            dr[k] = tx[k] - sx[warp][k][jj];
+            rr += dr[k] * dr[k];
+          }
+          if (!(rr < a.dmax)) continue;
+          const T e = Real<T>::expm(rr * a.dinv);
+          if (CHG) {
+            // gnd_directc{p,g,h}, src/pfgt/pfgt_direct.f:47-196
+            T dg[DIM];
+#pragma unroll
+            for (int k = 0; k < DIM; k++) dg[k] = -a.rfac * dr[k];
+#pragma unroll
+            for (int i = 0; i < NDC; i++) {
+              if (i >= ndc) break;
+              const T r = e * sq[warp][i][jj];
+              acc[i][0] += r;
+              if (PGH >= 2)
+#pragma unroll
+                for (int k = 0; k < DIM; k++) acc[i][1 + k] += dg[k] * r;
+              if (PGH >= 3)
+#pragma unroll
+                for (int m = 0; m < NH; m++) {
+                  const int ka = HessIdx<DIM>::a(m), kb = HessIdx<DIM>::b(m);
+                  const T h = dg[ka] * dg[kb] + (ka == kb ? -a.rfac : T(0));
+                  acc[i][1 + DIM + m] += h * r;
+                }
+            }
+          }
+          if (DIP) {
+            // gnd_directd{p,g,h}, src/pfgt/pfgt_direct.f:204-384
+            T d[DIM], rn[DIM], rinc = T(0);
+#pragma unroll
+            for (int k = 0; k < DIM; k++) {
+              d[k] = a.rfac * dr[k];
+              rn[k] = sn[warp][k][jj];
+              rinc += d[k] * rn[k];
+            }
+            T rg[DIM];
+#pragma unroll
+            for (int k = 0; k < DIM; k++) rg[k] = rn[k] * a.rfac - rinc * d[k];
+#pragma unroll
+            for (int i = 0; i < NDC; i++) {
+              if (i >= ndc) break;
+              const T r = e * sd[warp][i][jj];
+              acc[i][0] += rinc * r;
+              if (PGH >= 2)
+#pragma unroll
+                for (int k = 0; k < DIM; k++) acc[i][1 + k] += rg[k] * r;
+              if (PGH >= 3)
+#pragma unroll
+                for (int m = 0; m < NH; m++) {
+                  const int ka = HessIdx<DIM>::a(m), kb = HessIdx<DIM>::b(m);
+                  T h = (ka == kb) ? (-a.rfac * (d[ka] * rn[ka] + rinc) - rg[ka] * d[ka])
+                                   : (-a.rfac * d[ka] * rn[kb] - rg[ka] * d[kb]);
+                  acc[i][1 + DIM + m] += h * r;
+                }
+            }
+          }
+        }
+      }
+    }
+    if (act) {
+#pragma unroll
+      for (int i = 0; i < NDC; i++) {
+        if (i >= ndc) break;
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          double* o = &a.out[((size_t)c * a.nd + a.d0 + i) * a.ne + p];
+          *o += (double)acc[i][c];
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_items_count(int nboxes, const int* __restrict__ l1_ptr, const int* __restrict__ lo,
+                              const int* __restrict__ hi, const int* __restrict__ s_lo,
+                              const int* __restrict__ s_hi, const int* __restrict__ l1_src,
+                              int* __restrict__ cnt, double* __restrict__ pairs) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nboxes; b += gridDim.x * blockDim.x) {
+    int ne = hi[b] - lo[b], nl = l1_ptr[b + 1] - l1_ptr[b];
+    cnt[b] = (ne > 0 && nl > 0) ? (ne + 31) / 32 : 0;
+    if (pairs && ne > 0 && nl > 0) {
+      double ns = 0;
+      for (int i = l1_ptr[b]; i < l1_ptr[b + 1]; i++) ns += s_hi[l1_src[i]] - s_lo[l1_src[i]];
+      atomicAdd(pairs, ns * ne);
+    }
+  }
+}
+__global__ void k_items_fill(int nboxes, const int* __restrict__ cnt, const int* __restrict__ pos,
+                             const int* __restrict__ lo, int* __restrict__ ibox,
+                             int* __restrict__ ilo) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nboxes; b += gridDim.x * blockDim.x)
+    for (int c = 0; c < cnt[b]; c++) {
+      ibox[pos[b] + c] = b;
+      ilo[pos[b] + c] = lo[b] + 32 * c;
+    }
+}
+
+template <typename T, int DIM, int PGH, bool CHG, bool DIP, int NDC>
+void launch_direct(const DArgs<T>& a, cudaStream_t s) {
+  int grid = std::max(1, std::min(ceil_div(a.n_items, DW), kSMs * 16));
+  k_direct<T, DIM, PGH, CHG, DIP, NDC><<<grid, DW * 32, 0, s>>>(a);
+  FGT_LAUNCH_CHECK();
+}
+
+template <typename T, int DIM, int PGH, int NDC>
+void dispatch_cd(const DArgs<T>& a, bool chg, bool dip, cudaStream_t s) {
+  if (chg && dip) launch_direct<T, DIM, PGH, true, true, NDC>(a, s);
+  else if (chg) launch_direct<T, DIM, PGH, true, false, NDC>(a, s);
+  else launch_direct<T, DIM, PGH, false, true, NDC>(a, s);
+}
+template <typename T, int DIM, int NDC>
+void dispatch_pgh(const DArgs<T>& a, int pgh, bool chg, bool dip, cudaStream_t s) {
+  if (pgh == 1) dispatch_cd<T, DIM, 1, NDC>(a, chg, dip, s);
+  else if (pgh == 2) dispatch_cd<T, DIM, 2, NDC>(a, chg, dip, s);
+  else dispatch_cd<T, DIM, 3, NDC>(a, chg, dip, s);
+}
+template <typename T, int NDC>
+void dispatch_dim(const DArgs<T>& a, int dim, int pgh, bool chg, bool dip, cudaStream_t s) {
+  if (dim == 1) dispatch_pgh<T, 1, NDC>(a, pgh, chg, dip, s);
+  else if (dim == 2) dispatch_pgh<T, 2, NDC>(a, pgh, chg, dip, s);
+  else dispatch_pgh<T, 3, NDC>(a, pgh, chg, dip, s);
+}
+
+}  // namespace
+
+template <typename T>
+int direct_near_field(const DirectGeom& g, const Lists& L, const SourceSet<T>& src,
+                      const EvalSet<T>& e, double* pairs, cudaStream_t s) {
+  if (e.pgh <= 0 || e.n <= 0 || L.n_l1 <= 0) return 0;
+  int nb = g.nboxes, launches = 0;
+  DBuf<int> cnt(nb, s), pos(nb, s), tot(1, s);
+  DBuf<double> dpairs(1, s);
+  dpairs.zero();
+  k_items_count<<<grid_for(nb, 128), 128, 0, s>>>(nb, L.l1_ptr, e.lo, e.hi, src.lo, src.hi,
+                                                   L.l1_src, cnt, pairs ? dpairs.get() : nullptr);
+  FGT_LAUNCH_CHECK();
+  exclusive_scan_i32(cnt, pos, nb, tot, s);
+  int n_items = fetch_int(tot, s);
+  if (pairs) {
+    double h = 0;
+    FGT_CUDA(cudaMemcpyAsync(&h, dpairs.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+    FGT_CUDA(cudaStreamSynchronize(s));
+    *pairs += h;
+  }
+  launches += 2;
+  if (n_items == 0) return launches;
+  DBuf<int> ibox(n_items, s), ilo(n_items, s);
+  k_items_fill<<<grid_for(nb, 128), 128, 0, s>>>(nb, cnt, pos, e.lo, ibox, ilo);
+  FGT_LAUNCH_CHECK();
+  launches++;
+  DArgs<T> a;
+  a.n_items = n_items;
+  a.nd = g.nd;
+  a.ne = e.n;
+  a.ns = src.n;
+  a.iperiod0 = g.iperiod0;
+  a.dinv = (T)(1.0 / g.delta);
+  a.dmax = (T)g.dmax;
+  a.rfac = (T)(2.0 / g.delta);
+  a.bs0 = g.bs0;
+  a.item_box = ibox;
+  a.item_lo = ilo;
+  a.l1_ptr = L.l1_ptr;
+  a.l1_src = L.l1_src;
+  a.s_lo = src.lo;
+  a.s_hi = src.hi;
+  a.e_hi = e.hi;
+  a.soff = src.off;
+  a.q = src.q;
+  a.ds = src.ds;
+  a.rn = src.rn;
+  a.eoff = e.off;
+  a.center = g.center;
+  a.out = e.out;
+  bool chg = src.q != nullptr, dip = src.ds != nullptr;
+  for (int d0 = 0; d0 < g.nd; d0 += (g.nd == 1 ? 1 : 4)) {
+    a.d0 = d0;
+    if (g.nd == 1) dispatch_dim<T, 1>(a, g.dim, e.pgh, chg, dip, s);
+    else dispatch_dim<T, 4>(a, g.dim, e.pgh, chg, dip, s);
+    launches++;
+  }
+  return launches;
+}
+
+template int direct_near_field<float>(const DirectGeom&, const Lists&, const SourceSet<float>&,
+                                      const EvalSet<float>&, double*, cudaStream_t);
+template int direct_near_field<double>(const DirectGeom&, const Lists&, const SourceSet<double>&,
+                                       const EvalSet<double>&, double*, cudaStream_t);
+
+}  // namespace fgt
+
+// ---------------------------------------------------------------------------
+// All-pairs FP64 direct sum with the argument list of the reference's
+// pfgt_direct (src/pfgt/pfgt.f:1156-1382): used by the pfgt_direct_ export.
+namespace fgt {
+namespace {
+__global__ void k_direct_all(int nd, int dim, double delta, double dmax, const double* __restrict__ shift,
+                             int ns, const double* __restrict__ src, const double* __restrict__ q,
+                             const double* __restrict__ rn, const double* __restrict__ ds, int nt,
+                             const double* __restrict__ trg, int pgh, double* __restrict__ pot,
+                             double* __restrict__ grad, double* __restrict__ hess) {
+  const int nh = dim * (dim + 1) / 2;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nt; j += gridDim.x * blockDim.x) {
+    for (int i = 0; i < ns; i++) {
+      double dr[3], rr = 0;
+      for (int k = 0; k < dim; k++) {
+        dr[k] = trg[(size_t)j * dim + k] - (src[(size_t)i * dim + k] + (shift ? shift[k] : 0.0));
+        rr += dr[k] * dr[k];
+      }
+      if (!(rr < dmax)) continue;
+      double e = exp(-rr / delta);
+      int ha[6], hb[6];
+      if (dim == 1) { ha[0] = 0; hb[0] = 0; }
+      else if (dim == 2) { ha[0] = 0; hb[0] = 0; ha[1] = 0; hb[1] = 1; ha[2] = 1; hb[2] = 1; }
+      else {
+        ha[0] = 0; hb[0] = 0; ha[1] = 1; hb[1] = 1; ha[2] = 2; hb[2] = 2;
+        ha[3] = 0; hb[3] = 1; ha[4] = 0; hb[4] = 2; ha[5] = 1; hb[5] = 2;
+      }
+      if (q) {
+        double rf = -2.0 / delta, dg[3];
+        for (int k = 0; k < dim; k++) dg[k] = rf * dr[k];
+        for (int id = 0; id < nd; id++) {
+          double r = e * q[(size_t)i * nd + id];
+          pot[(size_t)j * nd + id] += r;
+          if (pgh >= 2)
+            for (int k = 0; k < dim; k++) grad[((size_t)j * dim + k) * nd + id] += dg[k] * r;
+          if (pgh >= 3)
+            for (int m = 0; m < nh; m++)
+              hess[((size_t)j * nh + m) * nd + id] +=
+                  (dg[ha[m]] * dg[hb[m]] + (ha[m] == hb[m] ? rf : 0.0)) * r;
+        }
+      }
+      if (ds) {
+        double rf = 2.0 / delta, d[3], n[3], rinc = 0, rg[3];
+        for (int k = 0; k < dim; k++) {
+          d[k] = rf * dr[k];
+          n[k] = rn[(size_t)i * dim + k];
+          rinc += d[k] * n[k];
+        }
+        for (int k = 0; k < dim; k++) rg[k] = n[k] * rf - rinc * d[k];
+        for (int id = 0; id < nd; id++) {
+          double r = e * ds[(size_t)i * nd + id];
+          pot[(size_t)j * nd + id] += rinc * r;
+          if (pgh >= 2)
+            for (int k = 0; k < dim; k++) grad[((size_t)j * dim + k) * nd + id] += rg[k] * r;
+          if (pgh >= 3)
+            for (int m = 0; m < nh; m++) {
+              int a = ha[m], b = hb[m];
+              double h = (a == b) ? (-rf * (d[a] * n[a] + rinc) - rg[a] * d[a])
+                                  : (-rf * d[a] * n[b] - rg[a] * d[b]);
+              hess[((size_t)j * nh + m) * nd + id] += h * r;
+            }
+        }
+      }
+    }
+  }
+}
+}  // namespace
+
+void direct_all_pairs(int nd, int dim, double delta, double dmax, const double* shift, int ns,
+                      const double* src, const double* q, const double* rn, const double* ds,
+                      int nt, const double* trg, int pgh, double* pot, double* grad, double* hess,
+                      cudaStream_t s) {
+  if (nt <= 0 || ns <= 0 || pgh <= 0) return;
+  k_direct_all<<<grid_for(nt, 128), 128, 0, s>>>(nd, dim, delta, dmax, shift, ns, src, q, rn, ds,
+                                                 nt, trg, pgh, pot, grad, hess);
+  FGT_LAUNCH_CHECK();
+}
+
+}  // namespace fgt

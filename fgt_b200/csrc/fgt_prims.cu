@@ -1,0 +1,224 @@
+// Scans, stable LSD radix sort and searches used by the tree build.
+#include "fgt_prims.cuh"
+
+namespace fgt {
+
+namespace {
+
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ int warp_incl_scan(int v) {
+  int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  return v;
+}
+
+// Exclusive block scan of one value per thread; returns block total.
+__device__ __forceinline__ int block_excl_scan(int v, int* total) {
+  __shared__ int ws[32];
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int inc = warp_incl_scan(v);
+  if (lane == 31) ws[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    int x = lane < nw ? ws[lane] : 0;
+    int xi = warp_incl_scan(x);
+    if (lane < nw) ws[lane] = xi - x;
+    if (lane == nw - 1) ws[31] = xi;
+  }
+  __syncthreads();
+  int r = inc - v + ws[w];
+  *total = ws[31];
+  __syncthreads();
+  return r;
+}
+
+__global__ void k_scan_reduce(const int* __restrict__ in, int n, int* __restrict__ part) {
+  int base = blockIdx.x * SCAN_TILE, s = 0;
+  for (int j = 0; j < SCAN_ITEMS; j++) {
+    int i = base + threadIdx.x * SCAN_ITEMS + j;
+    if (i < n) s += in[i];
+  }
+  int tot;
+  block_excl_scan(s, &tot);
+  if (threadIdx.x == 0) part[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_apply(const int* in, int* out, int n, const int* __restrict__ part,
+                             int* total, int nblocks) {
+  int base = blockIdx.x * SCAN_TILE;
+  int v[SCAN_ITEMS], s = 0;
+  for (int j = 0; j < SCAN_ITEMS; j++) {
+    int i = base + threadIdx.x * SCAN_ITEMS + j;
+    v[j] = (i < n) ? in[i] : 0;
+    s += v[j];
+  }
+  int tot;
+  int ex = block_excl_scan(s, &tot) + (part ? part[blockIdx.x] : 0);
+  for (int j = 0; j < SCAN_ITEMS; j++) {
+    int i = base + threadIdx.x * SCAN_ITEMS + j;
+    if (i < n) out[i] = ex;
+    ex += v[j];
+  }
+  if (total && blockIdx.x == nblocks - 1 && threadIdx.x == SCAN_THREADS - 1) *total = ex;
+}
+
+// ---------------------------------------------------------------- radix sort
+constexpr int RS_THREADS = 256;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+constexpr int RS_WARPS = RS_THREADS / 32;
+
+__global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const uint64_t* __restrict__ keys, int n,
+                                                           int shift, int* __restrict__ hist,
+                                                           int nblocks) {
+  __shared__ int h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  int base = blockIdx.x * RS_TILE;
+  for (int r = 0; r < RS_ITEMS; r++) {
+    int i = base + r * RS_THREADS + threadIdx.x;
+    if (i < n) atomicAdd(&h[(int)((keys[i] >> shift) & 255ull)], 1);
+  }
+  __syncthreads();
+  hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(RS_THREADS)
+    k_radix_scatter(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                    uint64_t* __restrict__ kout, uint32_t* __restrict__ vout, int n, int shift,
+                    const int* __restrict__ offs, int nblocks) {
+  __shared__ int base[256];
+  __shared__ int wc[RS_WARPS][256];
+  int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  base[tid] = offs[tid * nblocks + blockIdx.x];
+  unsigned lt = (1u << lane) - 1u;
+  int tbase = blockIdx.x * RS_TILE;
+  __syncthreads();
+  for (int r = 0; r < RS_ITEMS; r++) {
+    int i = tbase + r * RS_THREADS + tid;
+    bool valid = i < n;
+    uint64_t k = valid ? kin[i] : 0ull;
+    uint32_t v = (valid && vin) ? vin[i] : 0u;
+    int d = valid ? (int)((k >> shift) & 255ull) : 256;
+    unsigned peers = __match_any_sync(0xffffffffu, d);
+    int rank = __popc(peers & lt);
+    bool leader = (__ffs(peers) - 1) == lane;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; w++) wc[w][tid] = 0;
+    __syncthreads();
+    if (valid && leader) wc[warp][d] = __popc(peers);
+    __syncthreads();
+    {
+      int run = base[tid];
+#pragma unroll
+      for (int w = 0; w < RS_WARPS; w++) {
+        int c = wc[w][tid];
+        wc[w][tid] = run;
+        run += c;
+      }
+      base[tid] = run;
+    }
+    __syncthreads();
+    if (valid) {
+      int pos = wc[warp][d] + rank;
+      kout[pos] = k;
+      if (vout) vout[pos] = v;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_lower_bound(const uint64_t* __restrict__ a, int n, const uint64_t* __restrict__ q,
+                              int m, int* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    out[i] = dev_lower_bound(a, n, q[i]);
+}
+
+__global__ void k_unique_flags(const uint64_t* __restrict__ a, int n, int* __restrict__ f) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    f[i] = (i == 0 || a[i] != a[i - 1]) ? 1 : 0;
+}
+__global__ void k_unique_scatter(const uint64_t* __restrict__ a, int n, const int* __restrict__ pos,
+                                 uint64_t* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (i == 0 || a[i] != a[i - 1]) out[pos[i]] = a[i];
+}
+
+}  // namespace
+
+void exclusive_scan_i32(const int* in, int* out, int n, int* total, cudaStream_t s) {
+  if (n <= 0) {
+    if (total) FGT_CUDA(cudaMemsetAsync(total, 0, sizeof(int), s));
+    return;
+  }
+  int nb = ceil_div(n, SCAN_TILE);
+  if (nb == 1) {
+    k_scan_apply<<<1, SCAN_THREADS, 0, s>>>(in, out, n, nullptr, total, 1);
+    FGT_LAUNCH_CHECK();
+    return;
+  }
+  DBuf<int> part(nb, s);
+  k_scan_reduce<<<nb, SCAN_THREADS, 0, s>>>(in, n, part);
+  FGT_LAUNCH_CHECK();
+  exclusive_scan_i32(part, part, nb, nullptr, s);
+  k_scan_apply<<<nb, SCAN_THREADS, 0, s>>>(in, out, n, part, total, nb);
+  FGT_LAUNCH_CHECK();
+}
+
+void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* ktmp, uint32_t* vtmp, int n, int bits,
+                cudaStream_t s) {
+  if (n <= 1 || bits <= 0) return;
+  int nb = ceil_div(n, RS_TILE);
+  DBuf<int> hist((size_t)256 * nb, s);
+  uint64_t *ka = keys, *kb = ktmp;
+  uint32_t *va = vals, *vb = vtmp;
+  int passes = 0;
+  for (int shift = 0; shift < bits; shift += 8) {
+    k_radix_hist<<<nb, RS_THREADS, 0, s>>>(ka, n, shift, hist, nb);
+    FGT_LAUNCH_CHECK();
+    exclusive_scan_i32(hist, hist, 256 * nb, nullptr, s);
+    k_radix_scatter<<<nb, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, shift, hist, nb);
+    FGT_LAUNCH_CHECK();
+    std::swap(ka, kb);
+    std::swap(va, vb);
+    passes++;
+  }
+  if (passes & 1) {
+    FGT_CUDA(cudaMemcpyAsync(keys, ka, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, s));
+    if (vals) FGT_CUDA(cudaMemcpyAsync(vals, va, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+  }
+}
+
+void lower_bound_u64(const uint64_t* sorted, int n, const uint64_t* q, int m, int* out,
+                     cudaStream_t s) {
+  if (m <= 0) return;
+  k_lower_bound<<<grid_for(m, 256), 256, 0, s>>>(sorted, n, q, m, out);
+  FGT_LAUNCH_CHECK();
+}
+
+int fetch_int(const int* d, cudaStream_t s) {
+  int h = 0;
+  FGT_CUDA(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FGT_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+int unique_sorted_u64(const uint64_t* in, int n, uint64_t* out, cudaStream_t s) {
+  if (n <= 0) return 0;
+  DBuf<int> f(n, s), tot(1, s);
+  k_unique_flags<<<grid_for(n, 256), 256, 0, s>>>(in, n, f);
+  FGT_LAUNCH_CHECK();
+  exclusive_scan_i32(f, f, n, tot, s);
+  k_unique_scatter<<<grid_for(n, 256), 256, 0, s>>>(in, n, f, out);
+  FGT_LAUNCH_CHECK();
+  return fetch_int(tot, s);
+}
+
+}  // namespace fgt

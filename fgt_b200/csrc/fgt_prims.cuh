@@ -1,0 +1,87 @@
+// Device primitives: stream-ordered buffers, scans, a stable LSD radix sort,
+// sorted-array searches.  All hand-written; no CUB/Thrust.
+#pragma once
+#include "fgt_common.cuh"
+
+namespace fgt {
+
+// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync).
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaStream_t s = 0;
+  DBuf() = default;
+  DBuf(size_t count, cudaStream_t st) { alloc(count, st); }
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p; n = o.n; s = o.s;
+      o.p = nullptr; o.n = 0;
+    }
+    return *this;
+  }
+  void alloc(size_t count, cudaStream_t st) {
+    release();
+    s = st;
+    n = count;
+    size_t bytes = (count ? count : 1) * sizeof(T);
+    cudaError_t e = cudaMallocAsync((void**)&p, bytes, st);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      (void)cudaGetLastError();
+      fgt_set_error_message("device allocation failed", __FILE__, __LINE__);
+      throw Error{FGT_ERR_NOMEM, "device allocation failed"};
+    }
+  }
+  void zero() {
+    if (p) FGT_CUDA(cudaMemsetAsync(p, 0, (n ? n : 1) * sizeof(T), s));
+  }
+  void release() {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { release(); }
+  T* get() const { return p; }
+  operator T*() const { return p; }
+};
+
+// Exclusive prefix sum of n int32 values (in == out allowed).  If total is not
+// null, the grand total is written to *total (device pointer).
+void exclusive_scan_i32(const int* in, int* out, int n, int* total, cudaStream_t s);
+
+// Stable LSD radix sort on the low `bits` bits of 64-bit keys, carrying
+// optional 32-bit values.  Results end in keys/vals (tmp buffers of n).
+void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* ktmp, uint32_t* vtmp, int n,
+                int bits, cudaStream_t s);
+
+// out[i] = lower_bound(sorted, n, q[i]) for m queries.
+void lower_bound_u64(const uint64_t* sorted, int n, const uint64_t* q, int m, int* out,
+                     cudaStream_t s);
+
+// Compact the unique values of a sorted uint64 array; returns the count
+// (synchronises the stream).
+int unique_sorted_u64(const uint64_t* in, int n, uint64_t* out, cudaStream_t s);
+
+// Copy a device int to the host (synchronises the stream).
+int fetch_int(const int* d, cudaStream_t s);
+
+__device__ __forceinline__ int dev_lower_bound(const uint64_t* a, int n, uint64_t v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (a[mid] < v) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+// index of v in sorted a, or -1
+__device__ __forceinline__ int dev_find(const uint64_t* a, int n, uint64_t v) {
+  int i = dev_lower_bound(a, n, v);
+  return (i < n && a[i] == v) ? i : -1;
+}
+
+}  // namespace fgt

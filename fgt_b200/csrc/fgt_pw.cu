@@ -1,0 +1,1036 @@
+// Plane-wave form / translate / evaluate kernels (K6, K7, K8).
+//
+// Per box, one CTA keeps the whole spreading sub-grid in shared memory (a
+// global-memory slice per CTA when it does not fit): spread (ES kernel,
+// Barnett-Magland-af Klinteberg 2019) -> in-place pruned DFT passes along the
+// last, middle and first dimension -> deconvolution and PW weights fused into
+// the pass that writes the expansion.  Only the sub-grid the box's points can
+// reach is stored: for boxes of the cut-off size the scaled coordinates lie
+// in [-pi/3, pi/3], about a third of the 2*pi period.
+#include <math.h>
+
+#include <algorithm>
+#include <complex>
+#include <vector>
+
+#include "fgt_pw.cuh"
+
+namespace fgt {
+
+namespace {
+
+constexpr int PW_THREADS = 256;
+constexpr int MAXSMEM = 227 * 1024;
+
+struct Geo {
+  int dim, K, G, l0, nf, wrap, nexp, nd;
+  int S[3], str[3];  // buffer extents and strides (T units) per dim
+  int bufsz;
+};
+
+template <typename T>
+struct PWArgs {
+  Geo g;
+  T scale, inv_dx, halfw_over_dx, beta, inv_halfw, dx, l0dx;
+  const T* twf;  // [G][2K+1] fwd full
+  const T* twh;  // [G][K+1]  fwd half
+  const T* tif;  // [2K+1][G] inv full
+  const T* tih;  // [K+1][G]  inv half (with 1/2/2/.. weights)
+  const T* facf; // [2K+1] dx*wsym/phihat
+  const T* faci; // [2K+1] dx/phihat
+  const T* ts;   // [2K+1] ts(k)
+  T inv_sqd0;
+  T* gscratch;   // global buffer slices when the grid does not fit in smem
+};
+
+// ---------------------------------------------------------------- passes
+// In-place line transforms over whole lines per round (a line is read
+// completely before any of its outputs is written).
+// MODE 0: real -> half complex (fwd, last dim), MODE 1: complex -> complex,
+// MODE 2: half complex -> real (inv, last dim).
+template <typename T, int MODE>
+__device__ __forceinline__ void pass_inplace(T* B, int nl, int nb, int SA, int SB, int ein,
+                                             int eout, int nin, int nout, const T* __restrict__ tw) {
+  const int lpr = blockDim.x / nout;
+  const int t = threadIdx.x, lo = t / nout, k = t - lo * nout;
+  const bool act_t = lo < lpr;
+  for (int l0 = 0; l0 < nl; l0 += lpr) {
+    const int line = l0 + lo;
+    const bool act = act_t && line < nl;
+    T re = T(0), im = T(0);
+    int base = 0;
+    if (act) {
+      base = (line / nb) * SA + (line % nb) * SB;
+      for (int l = 0; l < nin; l++) {
+        const T twr = tw[2 * (l * nout + k)], twi = tw[2 * (l * nout + k) + 1];
+        if (MODE == 0) {
+          const T gv = B[base + l * ein];
+          re += gv * twr;
+          im += gv * twi;
+        } else {
+          const T xr = B[base + l * ein], xi = B[base + l * ein + 1];
+          re += xr * twr - xi * twi;
+          if (MODE == 1) im += xr * twi + xi * twr;
+        }
+      }
+    }
+    __syncthreads();
+    if (act) {
+      if (MODE == 2) {
+        B[base + k * eout] = re;
+      } else {
+        B[base + k * eout] = re;
+        B[base + k * eout + 1] = im;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ES kernel value at offset t (grid units relative to the point).
+template <typename T>
+__device__ __forceinline__ T es_kernel(T z, T beta) {
+  T u = T(1) - z * z;
+  u = u > T(0) ? u : T(0);
+  return Real<T>::expm(beta * (T(1) - Real<T>::sqrt_(u)));
+}
+
+// First cell and kernel values of one coordinate.
+template <typename T, int W>
+__device__ __forceinline__ int kernel_row(const PWArgs<T>& a, T x, T* phi) {
+  // cells i0..i0+W-1 with i0 = ceil((x - halfw)/dx)
+  const T u = x * a.inv_dx;
+  const int i0 = (int)ceil(u - a.halfw_over_dx);
+#pragma unroll
+  for (int j = 0; j < W; j++) {
+    const T z = ((T)(i0 + j) - u) / a.halfw_over_dx;
+    phi[j] = es_kernel<T>(z, a.beta);
+  }
+  return i0;
+}
+
+template <typename T, int W>
+__device__ __forceinline__ void cell_index(const Geo& g, int i0, int* idx) {
+  // local cell indices (wrapped on the full periodic grid)
+  if (g.wrap) {
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+      int c = (i0 + j) % g.nf;
+      idx[j] = c < 0 ? c + g.nf : c;
+    }
+  } else {
+    int b = i0 - g.l0;
+    b = b < 0 ? 0 : (b > g.G - W ? g.G - W : b);
+#pragma unroll
+    for (int j = 0; j < W; j++) idx[j] = b + j;
+  }
+}
+
+template <typename T, int DIM, int W>
+__device__ __forceinline__ void spread_point(const PWArgs<T>& a, T* B, const T* x, T str) {
+  const Geo& g = a.g;
+  if (DIM == 1) {
+    T px[W];
+    int ix[W];
+    cell_index<T, W>(g, kernel_row<T, W>(a, x[0], px), ix);
+#pragma unroll
+    for (int j = 0; j < W; j++) atomicAdd(&B[ix[j]], str * px[j]);
+  } else if (DIM == 2) {
+    T px[W], py[W];
+    int ix[W], iy[W];
+    cell_index<T, W>(g, kernel_row<T, W>(a, x[0], px), ix);
+    cell_index<T, W>(g, kernel_row<T, W>(a, x[1], py), iy);
+#pragma unroll 1
+    for (int jx = 0; jx < W; jx++) {
+      const T v = str * px[jx];
+      const int bx = ix[jx] * g.str[0];
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) atomicAdd(&B[bx + iy[jy]], v * py[jy]);
+    }
+  } else {
+    T py[W], pz[W];
+    int ix[W], iy[W], iz[W];
+    T px[W];
+    cell_index<T, W>(g, kernel_row<T, W>(a, x[0], px), ix);
+    cell_index<T, W>(g, kernel_row<T, W>(a, x[1], py), iy);
+    cell_index<T, W>(g, kernel_row<T, W>(a, x[2], pz), iz);
+#pragma unroll 1
+    for (int jx = 0; jx < W; jx++) {
+      const T vx = str * px[jx];
+      const int bx = ix[jx] * g.str[0];
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        const T vxy = vx * py[jy];
+        const int bxy = bx + iy[jy] * g.str[1];
+#pragma unroll
+        for (int jz = 0; jz < W; jz++) atomicAdd(&B[bxy + iz[jz]], vxy * pz[jz]);
+      }
+    }
+  }
+}
+
+template <typename T, int DIM, int W>
+__device__ __forceinline__ T interp_point(const PWArgs<T>& a, const T* B, const T* x) {
+  const Geo& g = a.g;
+  T acc = T(0);
+  if (DIM == 1) {
+    T px[W];
+    int ix[W];
+    cell_index<T, W>(g, kernel_row<T, W>(a, x[0], px), ix);
+#pragma unroll
+    for (int j = 0; j < W; j++) acc += B[ix[j]] * px[j];
+  } else if (DIM == 2) {
+    T px[W], py[W];
+    int ix[W], iy[W];
+    cell_index<T, W>(g, kernel_row<T, W>(a, x[0], px), ix);
+    cell_index<T, W>(g, kernel_row<T, W>(a, x[1], py), iy);
+#pragma unroll 1
+    for (int jx = 0; jx < W; jx++) {
+      const int bx = ix[jx] * g.str[0];
+      T s = T(0);
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) s += B[bx + iy[jy]] * py[jy];
+      acc += s * px[jx];
+    }
+  } else {
+    T px[W], py[W], pz[W];
+    int ix[W], iy[W], iz[W];
+    cell_index<T, W>(g, kernel_row<T, W>(a, x[0], px), ix);
+    cell_index<T, W>(g, kernel_row<T, W>(a, x[1], py), iy);
+    cell_index<T, W>(g, kernel_row<T, W>(a, x[2], pz), iz);
+#pragma unroll 1
+    for (int jx = 0; jx < W; jx++) {
+      const int bx = ix[jx] * g.str[0];
+      T sx = T(0);
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        const int bxy = bx + iy[jy] * g.str[1];
+        T sy = T(0);
+#pragma unroll
+        for (int jz = 0; jz < W; jz++) sy += B[bxy + iz[jz]] * pz[jz];
+        sx += sy * py[jy];
+      }
+      acc += sx * px[jx];
+    }
+  }
+  return acc;
+}
+
+template <typename T>
+__device__ __forceinline__ void load_tw(T* dst, const T* src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------- form
+struct FormIO {
+  int n_form, ns, nd, ncomp;  // ncomp: charge (1) and/or dipole (dim)
+  int has_q, has_dip;
+  const int *form_box, *s_lo, *s_hi;
+};
+
+template <typename T>
+struct FormPtrs {
+  const T *off, *q, *ds, *rn;  // sorted SoA
+  T* mp;                       // [n_form][nd][nexp] complex
+};
+
+template <typename T, int DIM, int W, bool GB>
+__global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, FormPtrs<T> p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Geo& g = a.g;
+  const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  T* twf = sm;                    // G*NF complex
+  T* twh = twf + 2 * G * NF;      // G*NH complex
+  T* B = GB ? a.gscratch + (size_t)blockIdx.x * g.bufsz : (twh + 2 * G * NH);
+  load_tw(twf, a.twf, 2 * G * NF);
+  load_tw(twh, a.twh, 2 * G * NH);
+  __syncthreads();
+  for (int fb = blockIdx.x; fb < io.n_form; fb += gridDim.x) {
+    const int box = io.form_box[fb];
+    const int p0 = io.s_lo[box], p1 = io.s_hi[box];
+    for (int id = 0; id < io.nd; id++) {
+      T* mp = p.mp + ((size_t)fb * io.nd + id) * 2 * g.nexp;
+      int first = 1;
+      for (int comp = 0; comp < io.ncomp; comp++) {
+        // comp 0 = charge when present; the others are dipole directions
+        const bool is_q = io.has_q && comp == 0;
+        const int dd = is_q ? -1 : comp - io.has_q;
+        for (int i = threadIdx.x; i < g.bufsz; i += blockDim.x) B[i] = T(0);
+        __syncthreads();
+        for (int pt = p0 + threadIdx.x; pt < p1; pt += blockDim.x) {
+          T x[DIM];
+#pragma unroll
+          for (int k = 0; k < DIM; k++) x[k] = p.off[(size_t)k * io.ns + pt] * a.scale;
+          T str = is_q ? p.q[(size_t)id * io.ns + pt]
+                       : p.ds[(size_t)id * io.ns + pt] * p.rn[(size_t)dd * io.ns + pt];
+          spread_point<T, DIM, W>(a, B, x, str);
+        }
+        __syncthreads();
+        // passes on the last and middle dimensions
+        if (DIM == 3) {
+          pass_inplace<T, 0>(B, G * G, G, g.str[0], g.str[1], 1, 2, G, NH, twh);
+          pass_inplace<T, 1>(B, G * NH, NH, g.str[0], 2, g.str[1], g.str[1], G, NF, twf);
+        } else if (DIM == 2) {
+          pass_inplace<T, 0>(B, G, 1, g.str[0], 0, 1, 2, G, NH, twh);
+        }
+        // final pass along x to the expansion, with weights and deconvolution
+        const int nline = DIM == 3 ? NF * NH : (DIM == 2 ? NH : 1);
+        const int nko = DIM == 1 ? NH : NF;
+        for (int o = threadIdx.x; o < nko * nline; o += blockDim.x) {
+          const int kxi = o / nline, line = o - kxi * nline;
+          int lb, kyi = 0, kz = 0;
+          if (DIM == 3) {
+            kyi = line / NH;
+            kz = line - kyi * NH;
+            lb = kyi * g.str[1] + 2 * kz;
+          } else if (DIM == 2) {
+            kz = line;
+            lb = 2 * line;
+          } else {
+            lb = 0;
+          }
+          T re = T(0), im = T(0);
+          if (DIM == 1) {
+            for (int l = 0; l < G; l++) {
+              const T gv = B[l];
+              re += gv * twh[2 * (l * NH + kxi)];
+              im += gv * twh[2 * (l * NH + kxi) + 1];
+            }
+          } else {
+            for (int l = 0; l < G; l++) {
+              const T xr = B[l * g.str[0] + lb], xi = B[l * g.str[0] + lb + 1];
+              const T tr = twf[2 * (l * NF + kxi)], ti = twf[2 * (l * NF + kxi) + 1];
+              re += xr * tr - xi * ti;
+              im += xr * ti + xi * tr;
+            }
+          }
+          // mode indices (k+K) per dimension; last dim stored k = 0..K
+          int ki[3];
+          if (DIM == 3) { ki[0] = kxi; ki[1] = kyi; ki[2] = kz + K; }
+          else if (DIM == 2) { ki[0] = kxi; ki[1] = kz + K; }
+          else { ki[0] = kxi + K; }
+          T f = T(1);
+#pragma unroll
+          for (int d = 0; d < DIM; d++) f *= a.facf[ki[d]];
+          T vr = re * f, vi = im * f;
+          if (!is_q) {  // * (-i) ts(k_d) / sqrt(delta0)
+            const T c = a.ts[ki[dd]] * a.inv_sqd0;
+            const T tr = vi * c, ti = -vr * c;
+            vr = tr;
+            vi = ti;
+          }
+          const int m = (DIM == 1) ? kxi : kxi * nline + line;
+          if (first) {
+            mp[2 * m] = vr;
+            mp[2 * m + 1] = vi;
+          } else {
+            mp[2 * m] += vr;
+            mp[2 * m + 1] += vi;
+          }
+        }
+        first = 0;
+        __syncthreads();
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- translate
+template <typename T>
+__global__ void k_translate(int n_eval, int nexp, int nd, const int* __restrict__ self,
+                            const int* __restrict__ ptr, const int* __restrict__ src,
+                            const int* __restrict__ widx, const T* __restrict__ mp,
+                            const T* __restrict__ wtab, T* __restrict__ loc) {
+  const int e = blockIdx.y;
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < nexp; m += gridDim.x * blockDim.x) {
+    for (int id = 0; id < nd; id++) {
+      T re = T(0), im = T(0);
+      const int sf = self[e];
+      if (sf >= 0) {
+        re = mp[(((size_t)sf * nd + id) * nexp + m) * 2];
+        im = mp[(((size_t)sf * nd + id) * nexp + m) * 2 + 1];
+      }
+      for (int j = ptr[e]; j < ptr[e + 1]; j++) {
+        const size_t mi = (((size_t)src[j] * nd + id) * nexp + m) * 2;
+        const size_t wi = ((size_t)widx[j] * nexp + m) * 2;
+        const T ar = mp[mi], ai = mp[mi + 1], wr = wtab[wi], wi_ = wtab[wi + 1];
+        re += ar * wr - ai * wi_;
+        im += ar * wi_ + ai * wr;
+      }
+      loc[(((size_t)e * nd + id) * nexp + m) * 2] = re;
+      loc[(((size_t)e * nd + id) * nexp + m) * 2 + 1] = im;
+    }
+  }
+}
+
+// W[s][m] = prod_d exp(i ts(k_d) xmin s_d) (gnd_mk_full_translation_matrices,
+// src/pfgt/pfgt_nufftrouts.f:336-424), s_d = s/3^d % 3 - 1.
+template <typename T>
+__global__ void k_wtab(int dim, int K, int nexp, const double* __restrict__ ts, double xmin,
+                       T* __restrict__ w) {
+  int nsh = dim == 1 ? 3 : (dim == 2 ? 9 : 27);
+  int NF = 2 * K + 1, NH = K + 1;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsh * nexp; i += gridDim.x * blockDim.x) {
+    int s = i / nexp, m = i - s * nexp;
+    int ki[3];
+    if (dim == 3) { ki[0] = m / (NF * NH); ki[1] = (m / NH) % NF; ki[2] = m % NH + K; }
+    else if (dim == 2) { ki[0] = m / NH; ki[1] = m % NH + K; }
+    else { ki[0] = m + K; }
+    double ph = 0;
+    int r = s;
+    for (int d = 0; d < dim; d++) {
+      int sd = r % 3 - 1;
+      r /= 3;
+      ph += ts[ki[d]] * xmin * sd;
+    }
+    double sn, cs;
+    sincos(ph, &sn, &cs);
+    w[2 * (size_t)i] = (T)cs;
+    w[2 * (size_t)i + 1] = (T)sn;
+  }
+}
+
+// ---------------------------------------------------------------- eval
+template <typename T>
+struct EvalPtrs {
+  const T* loc;  // [n_eval][nd][nexp]
+  const int* boxes;   // eval slots handled by this launch
+  const int* eval_box;
+  int nbox;
+  // two evaluation sets (sources, targets)
+  const T* off[2];
+  const int* lo[2];
+  const int* hi[2];
+  double* out[2];
+  int n[2], ncomp[2];
+  int nd, ncomp_max;
+};
+
+// component factor (complex) of evaluation component c at mode ki[]
+template <typename T, int DIM>
+__device__ __forceinline__ void eval_factor(const PWArgs<T>& a, int c, const int* ki, T& fr, T& fi) {
+  if (c == 0) { fr = T(1); fi = T(0); return; }
+  if (c <= DIM) {  // i ts(k_d)/sqrt(delta0)
+    fr = T(0);
+    fi = a.ts[ki[c - 1]] * a.inv_sqd0;
+    return;
+  }
+  int m = c - 1 - DIM, p, q;
+  if (DIM == 1) { p = 0; q = 0; }
+  else if (DIM == 2) { p = (m == 2) ? 1 : 0; q = (m == 0) ? 0 : 1; }
+  else { p = m < 3 ? m : (m < 5 ? 0 : 1); q = m < 3 ? m : (m == 3 ? 1 : 2); }
+  fr = -a.ts[ki[p]] * a.ts[ki[q]] * a.inv_sqd0 * a.inv_sqd0;
+  fi = T(0);
+}
+
+template <typename T, int DIM, int W, bool GB>
+__global__ void __launch_bounds__(PW_THREADS) k_eval_nufft(PWArgs<T> a, EvalPtrs<T> p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Geo& g = a.g;
+  const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  T* tif = sm;                 // NF*G complex
+  T* tih = tif + 2 * NF * G;   // NH*G complex
+  T* B = GB ? a.gscratch + (size_t)blockIdx.x * g.bufsz : (tih + 2 * NH * G);
+  load_tw(tif, a.tif, 2 * NF * G);
+  load_tw(tih, a.tih, 2 * NH * G);
+  __syncthreads();
+  for (int bi = blockIdx.x; bi < p.nbox; bi += gridDim.x) {
+    const int e = p.boxes[bi];
+    const int box = p.eval_box[e];
+    for (int id = 0; id < p.nd; id++) {
+      const T* L = p.loc + ((size_t)e * p.nd + id) * 2 * g.nexp;
+      for (int c = 0; c < p.ncomp_max; c++) {
+        // first pass (x) from the expansion into the grid buffer
+        const int nline = DIM == 3 ? NF * NH : (DIM == 2 ? NH : 1);
+        if (DIM == 1) {
+          for (int l = threadIdx.x; l < G; l += blockDim.x) {
+            T acc = T(0);
+            for (int k = 0; k < NH; k++) {
+              int ki[1] = {k + K};
+              T fr, fi;
+              eval_factor<T, DIM>(a, c, ki, fr, fi);
+              const T f = a.faci[k + K];
+              const T lr = L[2 * k] * f, li = L[2 * k + 1] * f;
+              const T mr = lr * fr - li * fi, mi = lr * fi + li * fr;
+              acc += mr * tih[2 * (k * G + l)] - mi * tih[2 * (k * G + l) + 1];
+            }
+            B[l] = acc;
+          }
+        } else {
+          for (int o = threadIdx.x; o < G * nline; o += blockDim.x) {
+            const int ix = o / nline, line = o - ix * nline;
+            int ki[3], lb;
+            if (DIM == 3) {
+              const int kyi = line / NH, kz = line - kyi * NH;
+              ki[1] = kyi;
+              ki[2] = kz + K;
+              lb = kyi * g.str[1] + 2 * kz;
+            } else {
+              ki[1] = line + K;
+              lb = 2 * line;
+            }
+            T fyz = T(1);
+#pragma unroll
+            for (int d = 1; d < DIM; d++) fyz *= a.faci[ki[d]];
+            T re = T(0), im = T(0);
+            for (int kxi = 0; kxi < NF; kxi++) {
+              ki[0] = kxi;
+              T fr, fi;
+              eval_factor<T, DIM>(a, c, ki, fr, fi);
+              const T f = fyz * a.faci[kxi];
+              const int m = kxi * nline + line;
+              const T lr = L[2 * m] * f, li = L[2 * m + 1] * f;
+              const T mr = lr * fr - li * fi, mi = lr * fi + li * fr;
+              const T tr = tif[2 * (kxi * G + ix)], ti = tif[2 * (kxi * G + ix) + 1];
+              re += mr * tr - mi * ti;
+              im += mr * ti + mi * tr;
+            }
+            B[ix * g.str[0] + lb] = re;
+            B[ix * g.str[0] + lb + 1] = im;
+          }
+        }
+        __syncthreads();
+        if (DIM == 3) {
+          pass_inplace<T, 1>(B, G * NH, NH, g.str[0], 2, g.str[1], g.str[1], NF, G, tif);
+          pass_inplace<T, 2>(B, G * G, G, g.str[0], g.str[1], 2, 1, NH, G, tih);
+        } else if (DIM == 2) {
+          pass_inplace<T, 2>(B, G, 1, g.str[0], 0, 2, 1, NH, G, tih);
+        }
+        // interpolate at the points of both evaluation sets
+        for (int set = 0; set < 2; set++) {
+          if (c >= p.ncomp[set] || p.n[set] == 0) continue;
+          const int q0 = p.lo[set][box], q1 = p.hi[set][box];
+          const int ne = p.n[set];
+          for (int pt = q0 + threadIdx.x; pt < q1; pt += blockDim.x) {
+            T x[DIM];
+#pragma unroll
+            for (int k = 0; k < DIM; k++) x[k] = p.off[set][(size_t)k * ne + pt] * a.scale;
+            const T v = interp_point<T, DIM, W>(a, B, x);
+            p.out[set][((size_t)c * p.nd + id) * ne + pt] += (double)v;
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void sincos_(float x, float* s, float* c) { sincosf(x, s, c); }
+__device__ __forceinline__ void sincos_(double x, double* s, double* c) { sincos(x, s, c); }
+
+// Direct modal evaluation for boxes with few points: one CTA per box, modes
+// split over threads, one block reduction per point.
+template <typename T, int DIM>
+__global__ void __launch_bounds__(PW_THREADS) k_eval_modal(PWArgs<T> a, EvalPtrs<T> p) {
+  const Geo& g = a.g;
+  const int K = g.K, NF = 2 * K + 1, NH = K + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* E = reinterpret_cast<T*>(smem_raw);  // [DIM][NF] complex e^{i k x_d}
+  __shared__ double red[PW_THREADS / 32][10];
+  const int nl = DIM == 3 ? NF * NH : (DIM == 2 ? NH : 1);
+  for (int bi = blockIdx.x; bi < p.nbox; bi += gridDim.x) {
+    const int e = p.boxes[bi];
+    const int box = p.eval_box[e];
+    for (int set = 0; set < 2; set++) {
+      if (p.n[set] == 0 || p.ncomp[set] == 0) continue;
+      const int q0 = p.lo[set][box], q1 = p.hi[set][box], ne = p.n[set], nc = p.ncomp[set];
+      for (int pt = q0; pt < q1; pt++) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < DIM * NF; i += blockDim.x) {
+          const int d = i / NF, k = i - d * NF - K;
+          const T x = p.off[set][(size_t)d * ne + pt] * a.scale;
+          T sn, cs;
+          sincos_(x * (T)k, &sn, &cs);
+          E[2 * i] = cs;
+          E[2 * i + 1] = sn;
+        }
+        __syncthreads();
+        for (int id = 0; id < p.nd; id++) {
+          const T* L = p.loc + ((size_t)e * p.nd + id) * 2 * g.nexp;
+          T acc[10];
+#pragma unroll
+          for (int c = 0; c < 10; c++) acc[c] = T(0);
+          for (int m = threadIdx.x; m < g.nexp; m += blockDim.x) {
+            int ki[3];
+            if (DIM == 3) { ki[0] = m / (NF * NH); ki[1] = (m / NH) % NF; ki[2] = m % NH + K; }
+            else if (DIM == 2) { ki[0] = m / NH; ki[1] = m % NH + K; }
+            else { ki[0] = m + K; }
+            T f = (ki[DIM - 1] == K) ? T(1) : T(2);  // Hermitian half-space weight
+            T er = T(1), ei = T(0);
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+              const T cr = E[2 * (d * NF + ki[d])], ci = E[2 * (d * NF + ki[d]) + 1];
+              const T nr = er * cr - ei * ci;
+              ei = er * ci + ei * cr;
+              er = nr;
+            }
+            const T lr = L[2 * m] * f, li = L[2 * m + 1] * f;
+            const T tr = lr * er - li * ei, ti = lr * ei + li * er;  // term = L e^{ikx}
+            acc[0] += tr;
+            if (nc > 1)
+#pragma unroll
+              for (int d = 0; d < DIM; d++) acc[1 + d] += -ti * a.ts[ki[d]] * a.inv_sqd0;
+            if (nc > 1 + DIM) {
+              const int nh = DIM * (DIM + 1) / 2;
+#pragma unroll
+              for (int hm = 0; hm < nh; hm++) {
+                int pp, qq;
+                if (DIM == 1) { pp = 0; qq = 0; }
+                else if (DIM == 2) { pp = (hm == 2) ? 1 : 0; qq = (hm == 0) ? 0 : 1; }
+                else { pp = hm < 3 ? hm : (hm < 5 ? 0 : 1); qq = hm < 3 ? hm : (hm == 3 ? 1 : 2); }
+                acc[1 + DIM + hm] += -tr * a.ts[ki[pp]] * a.ts[ki[qq]] * a.inv_sqd0 * a.inv_sqd0;
+              }
+            }
+          }
+          // block reduction of nc values
+          const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+          for (int c = 0; c < nc; c++) {
+            double v = (double)acc[c];
+            for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[w][c] = v;
+          }
+          __syncthreads();
+          if (threadIdx.x < nc) {
+            double v = 0;
+            for (int j = 0; j < (int)(blockDim.x >> 5); j++) v += red[j][threadIdx.x];
+            p.out[set][((size_t)threadIdx.x * p.nd + id) * ne + pt] += v;
+          }
+          __syncthreads();
+        }
+      }
+    }
+  }
+}
+
+// box partition by evaluation-point count
+__global__ void k_eval_split(int n_eval, const int* __restrict__ eval_box, const int* __restrict__ lo0,
+                             const int* __restrict__ hi0, const int* __restrict__ lo1,
+                             const int* __restrict__ hi1, int thr, int* __restrict__ big) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_eval; e += gridDim.x * blockDim.x) {
+    int b = eval_box[e];
+    int n = (lo0 ? hi0[b] - lo0[b] : 0) + (lo1 ? hi1[b] - lo1[b] : 0);
+    big[e] = n > thr ? 1 : 0;
+  }
+}
+__global__ void k_split_fill(int n, const int* __restrict__ f, const int* __restrict__ pos,
+                             int* __restrict__ big_list, int* __restrict__ small_list) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    if (f[e]) big_list[pos[e]] = e;
+    else small_list[e - pos[e]] = e;
+  }
+}
+
+int supported_w(int w) {
+  const int ws[] = {6, 8, 10, 12, 14, 16};
+  for (int v : ws)
+    if (w <= v) return v;
+  return 16;
+}
+
+template <typename T>
+struct DevTables {
+  DBuf<T> twf, twh, tif, tih, facf, faci, ts;
+  DBuf<double> ts64;
+};
+
+template <typename T>
+void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s) {
+  Geo& g = a.g;
+  g.dim = P.dim;
+  g.K = P.K;
+  g.G = P.G;
+  g.l0 = P.l0;
+  g.nf = P.nf;
+  g.wrap = P.wrap ? 1 : 0;
+  g.nexp = P.nexp;
+  g.nd = P.nd;
+  const int K = P.K, NF = 2 * K + 1, NH = K + 1, G = P.G;
+  int S[3] = {1, 1, 1};
+  if (P.dim == 3) {
+    S[0] = std::max(G, NF);
+    S[1] = std::max(G, NF);
+    S[2] = std::max(G, 2 * NH);
+  } else if (P.dim == 2) {
+    S[0] = std::max(G, NF);
+    S[1] = std::max(G, 2 * NH);
+  } else {
+    S[0] = std::max(G, 2 * NH);
+  }
+  g.bufsz = 1;
+  for (int d = 0; d < P.dim; d++) g.bufsz *= S[d];
+  for (int d = 0; d < 3; d++) g.S[d] = S[d];
+  g.str[P.dim - 1] = 1;
+  for (int d = P.dim - 2; d >= 0; d--) g.str[d] = g.str[d + 1] * S[d + 1];
+  a.scale = (T)(P.hpw / P.sqd0);
+  a.inv_dx = (T)(1.0 / P.dx);
+  a.halfw_over_dx = (T)(P.halfw / P.dx);
+  a.beta = (T)P.beta;
+  a.inv_halfw = (T)(1.0 / P.halfw);
+  a.dx = (T)P.dx;
+  a.l0dx = (T)(P.l0 * P.dx);
+  a.inv_sqd0 = (T)(1.0 / P.sqd0);
+  std::vector<T> twf(2 * G * NF), twh(2 * G * NH), tif(2 * NF * G), tih(2 * NH * G);
+  for (int l = 0; l < G; l++) {
+    double xl = (double)(P.l0 + l) * P.dx;
+    for (int k = -K; k <= K; k++) {
+      double c = cos(k * xl), sn = sin(k * xl);
+      twf[2 * (l * NF + k + K)] = (T)c;
+      twf[2 * (l * NF + k + K) + 1] = (T)(-sn);
+      tif[2 * ((k + K) * G + l)] = (T)c;
+      tif[2 * ((k + K) * G + l) + 1] = (T)sn;
+      if (k >= 0) {
+        twh[2 * (l * NH + k)] = (T)c;
+        twh[2 * (l * NH + k) + 1] = (T)(-sn);
+        double f = k == 0 ? 1.0 : 2.0;
+        tih[2 * (k * G + l)] = (T)(f * c);
+        tih[2 * (k * G + l) + 1] = (T)(f * sn);
+      }
+    }
+  }
+  std::vector<T> facf(NF), faci(NF), ts(NF);
+  for (int k = 0; k < NF; k++) {
+    facf[k] = (T)(P.dx * P.wsym[k] / P.phihat[k]);
+    faci[k] = (T)(P.dx / P.phihat[k]);
+    ts[k] = (T)P.ts[k];
+  }
+  auto up = [&](DBuf<T>& b, const std::vector<T>& h) {
+    b.alloc(h.size(), s);
+    FGT_CUDA(cudaMemcpyAsync(b.get(), h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
+  };
+  up(tb.twf, twf);
+  up(tb.twh, twh);
+  up(tb.tif, tif);
+  up(tb.tih, tih);
+  up(tb.facf, facf);
+  up(tb.faci, faci);
+  up(tb.ts, ts);
+  tb.ts64.alloc(NF, s);
+  FGT_CUDA(cudaMemcpyAsync(tb.ts64.get(), P.ts.data(), sizeof(double) * NF, cudaMemcpyHostToDevice, s));
+  FGT_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
+  a.twf = tb.twf;
+  a.twh = tb.twh;
+  a.tif = tb.tif;
+  a.tih = tb.tih;
+  a.facf = tb.facf;
+  a.faci = tb.faci;
+  a.ts = tb.ts;
+  a.gscratch = nullptr;
+}
+
+template <typename T>
+size_t tw_bytes(const PWArgs<T>& a) {
+  const int K = a.g.K, G = a.g.G;
+  return sizeof(T) * 2 * (size_t)G * ((2 * K + 1) + (K + 1));
+}
+
+template <typename KernelT>
+void set_smem(KernelT k, size_t bytes) {
+  FGT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+template <typename T, int DIM, int W>
+int launch_form(PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>& gs, cudaStream_t s) {
+  size_t tw = tw_bytes(a);
+  size_t need = tw + sizeof(T) * (size_t)a.g.bufsz;
+  int grid = std::max(1, std::min(io.n_form, kSMs * 2));
+  if (need <= (size_t)MAXSMEM) {
+    auto k = k_form<T, DIM, W, false>;
+    set_smem(k, need);
+    k<<<grid, PW_THREADS, need, s>>>(a, io, fp);
+  } else {
+    gs.alloc((size_t)grid * a.g.bufsz, s);
+    a.gscratch = gs;
+    auto k = k_form<T, DIM, W, true>;
+    set_smem(k, tw);
+    k<<<grid, PW_THREADS, tw, s>>>(a, io, fp);
+  }
+  FGT_LAUNCH_CHECK();
+  return 1;
+}
+
+template <typename T, int DIM, int W>
+int launch_eval(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t s) {
+  size_t tw = tw_bytes(a);
+  size_t need = tw + sizeof(T) * (size_t)a.g.bufsz;
+  int grid = std::max(1, std::min(ep.nbox, kSMs * 2));
+  if (need <= (size_t)MAXSMEM) {
+    auto k = k_eval_nufft<T, DIM, W, false>;
+    set_smem(k, need);
+    k<<<grid, PW_THREADS, need, s>>>(a, ep);
+  } else {
+    gs.alloc((size_t)grid * a.g.bufsz, s);
+    a.gscratch = gs;
+    auto k = k_eval_nufft<T, DIM, W, true>;
+    set_smem(k, tw);
+    k<<<grid, PW_THREADS, tw, s>>>(a, ep);
+  }
+  FGT_LAUNCH_CHECK();
+  return 1;
+}
+
+template <typename T, int DIM>
+int form_w(int w, PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>& gs, cudaStream_t s) {
+  switch (w) {
+    case 6: return launch_form<T, DIM, 6>(a, io, fp, gs, s);
+    case 8: return launch_form<T, DIM, 8>(a, io, fp, gs, s);
+    case 10: return launch_form<T, DIM, 10>(a, io, fp, gs, s);
+    case 12: return launch_form<T, DIM, 12>(a, io, fp, gs, s);
+    case 14: return launch_form<T, DIM, 14>(a, io, fp, gs, s);
+    default: return launch_form<T, DIM, 16>(a, io, fp, gs, s);
+  }
+}
+template <typename T, int DIM>
+int eval_w(int w, PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t s) {
+  switch (w) {
+    case 6: return launch_eval<T, DIM, 6>(a, ep, gs, s);
+    case 8: return launch_eval<T, DIM, 8>(a, ep, gs, s);
+    case 10: return launch_eval<T, DIM, 10>(a, ep, gs, s);
+    case 12: return launch_eval<T, DIM, 12>(a, ep, gs, s);
+    case 14: return launch_eval<T, DIM, 14>(a, ep, gs, s);
+    default: return launch_eval<T, DIM, 16>(a, ep, gs, s);
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host set-up
+void pw_setup(PWParams& P, int dim, int nd, int npw, double pmax, int periodic_nodes, double bs0,
+              double delta, double eps, double boxsize_cut, int spread_width) {
+  const double pi = 4.0 * atan(1.0);
+  P.dim = dim;
+  P.nd = nd;
+  P.K = npw / 2;
+  const int K = P.K, NF = 2 * K + 1;
+  P.nexp = dim == 3 ? NF * NF * (K + 1) : (dim == 2 ? NF * (K + 1) : K + 1);
+  double h;
+  P.ts.assign(NF, 0);
+  P.wsym.assign(NF, 0);
+  std::vector<double> ws(NF);
+  if (periodic_nodes) {
+    // get_periodic_pwnodes, src/common/fgtterms.f:191-211 (delta0 = 1)
+    h = 2 * pi / bs0;
+    double w = sqrt(pi * delta) / bs0, hw = h * sqrt(delta) / 2;
+    for (int k = -K; k <= K; k++) ws[k + K] = w * exp(-(hw * k) * (hw * k));
+    P.delta0 = 1.0;
+  } else {
+    // get_pwnodes (trapezoid), src/common/fgtterms.f:151-179
+    h = pmax / K;
+    double w = h / (2.0 * sqrt(pi));
+    for (int k = -K; k <= K; k++) {
+      double t = k * h;
+      ws[k + K] = w * exp(-t * t / 4);
+    }
+    P.delta0 = delta;
+  }
+  for (int k = -K; k <= K; k++) P.ts[k + K] = k * h;
+  for (int k = -K + 1; k <= K - 1; k++) P.wsym[k + K] = ws[k + K];
+  P.wsym[0] = P.wsym[2 * K] = ws[0] / 2;  // split the k=-K term over +-K
+  P.hpw = h;
+  P.sqd0 = sqrt(P.delta0);
+  P.xmin = boxsize_cut / P.sqd0;
+  // spreading grid (upsampling 2 over the 2K+1 modes), ES kernel
+  P.nf = 2 * NF + (2 * NF) % 2;
+  P.dx = 2 * pi / P.nf;
+  int w = spread_width > 0 ? spread_width : (int)ceil(log10(1.0 / eps)) + 2;
+  w = std::max(4, std::min(16, w));
+  w = supported_w(w);
+  P.w = w;
+  P.beta = 0.97 * pi * (1 - 1.0 / (2 * 2.0)) * w;
+  P.halfw = w * P.dx / 2;
+  double xmax = (boxsize_cut / 2) * (P.hpw / P.sqd0) * (1 + 1e-6) + 1e-12;
+  int lmin = (int)ceil((-xmax - P.halfw) / P.dx);
+  int lmax = (int)ceil((xmax - P.halfw) / P.dx) + w - 1;
+  P.l0 = lmin;
+  P.G = lmax - lmin + 1;
+  P.wrap = false;
+  if (P.G >= P.nf) {
+    P.wrap = true;
+    P.G = P.nf;
+    P.l0 = 0;
+  }
+  // every in-place pass round needs one whole line per thread group
+  FGT_REQUIRE(std::max(P.G, NF) <= PW_THREADS, FGT_ERR_UNSUPPORTED,
+              "plane-wave expansion too long for the spreading kernels");
+  // Fourier transform of the kernel, Gauss-Legendre on [0, halfw]
+  P.phihat.assign(NF, 0);
+  const int nq = 200;
+  std::vector<double> xq(nq), wq(nq);
+  for (int i = 0; i < nq; i++) {  // Newton on Legendre polynomials
+    double x = cos(pi * (i + 0.75) / (nq + 0.5));
+    for (int it = 0; it < 100; it++) {
+      double p0 = 1, p1 = x;
+      for (int j = 2; j <= nq; j++) {
+        double p2 = ((2 * j - 1) * x * p1 - (j - 1) * p0) / j;
+        p0 = p1;
+        p1 = p2;
+      }
+      double dp = nq * (x * p1 - p0) / (x * x - 1);
+      double dxn = p1 / dp;
+      x -= dxn;
+      if (fabs(dxn) < 1e-16) break;
+    }
+    double p0 = 1, p1 = x;
+    for (int j = 2; j <= nq; j++) {
+      double p2 = ((2 * j - 1) * x * p1 - (j - 1) * p0) / j;
+      p0 = p1;
+      p1 = p2;
+    }
+    double dp = nq * (x * p1 - p0) / (x * x - 1);
+    xq[i] = x;
+    wq[i] = 2 / ((1 - x * x) * dp * dp);
+  }
+  for (int k = -K; k <= K; k++) {
+    double acc = 0;
+    for (int i = 0; i < nq; i++) {
+      double t = xq[i] * P.halfw;  // over [-halfw, halfw]
+      double z = xq[i];
+      double ph = exp(P.beta * (sqrt(std::max(0.0, 1 - z * z)) - 1));
+      acc += wq[i] * P.halfw * ph * cos(k * t);
+    }
+    P.phihat[k + K] = acc;
+  }
+}
+
+// ------------------------------------------------------------------ drivers
+template <typename T>
+int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>& src,
+            PWData<T>& D, cudaStream_t s) {
+  if (L.n_form <= 0) {
+    D.mp.alloc(2, s);
+    return 0;
+  }
+  PWArgs<T> a;
+  DevTables<T> tb;
+  make_args<T>(P, a, tb, s);
+  D.mp.alloc((size_t)L.n_form * P.nd * 2 * P.nexp, s);
+  FormIO io;
+  io.n_form = L.n_form;
+  io.ns = src.n;
+  io.nd = P.nd;
+  io.has_q = src.q != nullptr;
+  io.has_dip = src.ds != nullptr;
+  io.ncomp = (io.has_q ? 1 : 0) + (io.has_dip ? P.dim : 0);
+  io.form_box = L.form_box;
+  io.s_lo = src.lo;
+  io.s_hi = src.hi;
+  FormPtrs<T> fp;
+  fp.off = src.off;
+  fp.q = src.q;
+  fp.ds = src.ds;
+  fp.rn = src.rn;
+  fp.mp = D.mp;
+  DBuf<T> gs;
+  int n;
+  if (P.dim == 1) n = form_w<T, 1>(P.w, a, io, fp, gs, s);
+  else if (P.dim == 2) n = form_w<T, 2>(P.w, a, io, fp, gs, s);
+  else n = form_w<T, 3>(P.w, a, io, fp, gs, s);
+  return n;
+}
+
+template <typename T>
+int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, cudaStream_t s) {
+  int nsh = P.dim == 1 ? 3 : (P.dim == 2 ? 9 : 27);
+  D.wtab.alloc((size_t)nsh * 2 * P.nexp, s);
+  DBuf<double> ts64(P.ts.size(), s);
+  FGT_CUDA(cudaMemcpyAsync(ts64.get(), P.ts.data(), sizeof(double) * P.ts.size(),
+                           cudaMemcpyHostToDevice, s));
+  k_wtab<T><<<grid_for((long long)nsh * P.nexp, 256), 256, 0, s>>>(P.dim, P.K, P.nexp, ts64,
+                                                                   P.xmin, D.wtab);
+  FGT_LAUNCH_CHECK();
+  D.loc.alloc((size_t)std::max(L.n_eval, 1) * P.nd * 2 * P.nexp, s);
+  if (L.n_eval == 0) return 1;
+  FGT_REQUIRE(L.n_eval < 65536 * 32, FGT_ERR_UNSUPPORTED, "too many expansion boxes");
+  int gx = std::max(1, std::min(ceil_div(P.nexp, 256), 64));
+  // grid.y limited to 65535: process in slabs
+  for (int e0 = 0; e0 < L.n_eval; e0 += 65535) {
+    int ne = std::min(65535, L.n_eval - e0);
+    dim3 grid(gx, ne);
+    k_translate<T><<<grid, 256, 0, s>>>(ne, P.nexp, P.nd, L.eval_self.get() + e0,
+                                        L.trans_ptr.get() + e0, L.trans_src, L.trans_w, D.mp,
+                                        D.wtab, D.loc.get() + (size_t)e0 * P.nd * 2 * P.nexp);
+    FGT_LAUNCH_CHECK();
+  }
+  FGT_CUDA(cudaStreamSynchronize(s));  // ts64 lifetime
+  return 2;
+}
+
+template <typename T>
+int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D,
+            const EvalSet<T>& e0, const EvalSet<T>& e1, int small_eval, int* n_nufft,
+            cudaStream_t s) {
+  // both evaluation sets (sources, targets) share the grid of every box
+  const bool u0 = e0.pgh > 0 && e0.n > 0, u1 = e1.pgh > 0 && e1.n > 0;
+  if (!(u0 || u1) || L.n_eval <= 0) return 0;
+  PWArgs<T> a;
+  DevTables<T> tb;
+  make_args<T>(P, a, tb, s);
+  int launches = 0;
+  const int thr = small_eval >= 0 ? small_eval : (P.dim == 3 ? 48 : (P.dim == 2 ? 8 : 4));
+  DBuf<int> big(L.n_eval, s), pos(L.n_eval, s), tot(1, s);
+  k_eval_split<<<grid_for(L.n_eval, 256), 256, 0, s>>>(
+      L.n_eval, L.eval_box, u0 ? e0.lo : nullptr, u0 ? e0.hi : nullptr, u1 ? e1.lo : nullptr,
+      u1 ? e1.hi : nullptr, thr, big);
+  FGT_LAUNCH_CHECK();
+  exclusive_scan_i32(big, pos, L.n_eval, tot, s);
+  int nbig = fetch_int(tot, s);
+  DBuf<int> lbig(std::max(nbig, 1), s), lsmall(std::max(L.n_eval - nbig, 1), s);
+  k_split_fill<<<grid_for(L.n_eval, 256), 256, 0, s>>>(L.n_eval, big, pos, lbig, lsmall);
+  FGT_LAUNCH_CHECK();
+  launches += 3;
+  int nh = P.dim * (P.dim + 1) / 2;
+  auto ncomp = [&](int pgh) { return pgh <= 0 ? 0 : 1 + (pgh >= 2 ? P.dim : 0) + (pgh >= 3 ? nh : 0); };
+  EvalPtrs<T> ep;
+  ep.loc = D.loc;
+  ep.eval_box = L.eval_box;
+  ep.nd = P.nd;
+  const EvalSet<T>* es[2] = {&e0, &e1};
+  bool us[2] = {u0, u1};
+  for (int i = 0; i < 2; i++) {
+    ep.off[i] = us[i] ? es[i]->off : nullptr;
+    ep.lo[i] = us[i] ? es[i]->lo : nullptr;
+    ep.hi[i] = us[i] ? es[i]->hi : nullptr;
+    ep.out[i] = us[i] ? es[i]->out : nullptr;
+    ep.n[i] = us[i] ? es[i]->n : 0;
+    ep.ncomp[i] = us[i] ? ncomp(es[i]->pgh) : 0;
+  }
+  ep.ncomp_max = std::max(ep.ncomp[0], ep.ncomp[1]);
+  DBuf<T> gs;
+  if (nbig > 0) {
+    ep.boxes = lbig;
+    ep.nbox = nbig;
+    if (P.dim == 1) launches += eval_w<T, 1>(P.w, a, ep, gs, s);
+    else if (P.dim == 2) launches += eval_w<T, 2>(P.w, a, ep, gs, s);
+    else launches += eval_w<T, 3>(P.w, a, ep, gs, s);
+    if (n_nufft) *n_nufft += nbig;
+  }
+  int nsmall = L.n_eval - nbig;
+  if (nsmall > 0) {
+    ep.boxes = lsmall;
+    ep.nbox = nsmall;
+    int grid = std::max(1, std::min(nsmall, kSMs * 8));
+    size_t sm = sizeof(T) * 2 * P.dim * (2 * P.K + 1);
+    if (P.dim == 1) k_eval_modal<T, 1><<<grid, PW_THREADS, sm, s>>>(a, ep);
+    else if (P.dim == 2) k_eval_modal<T, 2><<<grid, PW_THREADS, sm, s>>>(a, ep);
+    else k_eval_modal<T, 3><<<grid, PW_THREADS, sm, s>>>(a, ep);
+    FGT_LAUNCH_CHECK();
+    launches++;
+  }
+  FGT_CUDA(cudaStreamSynchronize(s));  // tables lifetime
+  return launches;
+}
+
+template int pw_form<float>(const PWParams&, const Tree&, const Lists&, const SourceSet<float>&,
+                            PWData<float>&, cudaStream_t);
+template int pw_form<double>(const PWParams&, const Tree&, const Lists&, const SourceSet<double>&,
+                             PWData<double>&, cudaStream_t);
+template int pw_translate<float>(const PWParams&, const Lists&, PWData<float>&, cudaStream_t);
+template int pw_translate<double>(const PWParams&, const Lists&, PWData<double>&, cudaStream_t);
+template int pw_eval<float>(const PWParams&, const Tree&, const Lists&, const PWData<float>&,
+                            const EvalSet<float>&, const EvalSet<float>&, int, int*, cudaStream_t);
+template int pw_eval<double>(const PWParams&, const Tree&, const Lists&, const PWData<double>&,
+                             const EvalSet<double>&, const EvalSet<double>&, int, int*,
+                             cudaStream_t);
+
+}  // namespace fgt

@@ -1,0 +1,155 @@
+/*
+ * fgt_b200.h -- C ABI of the B200 (sm_100a) discrete point fast Gauss
+ * transform.  Plain pointers and sizes only; no C++ or torch types.
+ *
+ * The drop-in entry point replaces the reference Fortran subroutine
+ *   subroutine pfgt(nd,dim,delta,eps,iperiod,bs0,cen0,ns,sources,
+ *                   ifcharge,charge,ifdipole,rnormal,dipstr,ifpgh,pot,grad,
+ *                   hess,nt,targ,ifpghtarg,pottarg,gradtarg,hesstarg)
+ * of src/pfgt/pfgt.f:6-10 (argument meaning: src/pfgt/pfgt.f:11-53).
+ *
+ * Array layouts are those of the reference (Fortran column-major, 4-byte
+ * integers): sources(dim,ns) -> sources[i*dim+k], charge(nd,ns) ->
+ * charge[i*nd+id], grad(nd,dim,n) -> grad[(i*dim+k)*nd+id],
+ * hess(nd,nhess,n) -> hess[(i*nhess+m)*nd+id], nhess = dim*(dim+1)/2, hessian
+ * order xx,yy,zz,xy,xz,yz (3D) and xx,xy,yy (2D) (src/pfgt/pfgt.f:52-53).
+ * Outputs are overwritten for the requested fields only; unrequested output
+ * arrays are never touched (length-1 dummies are fine), as in
+ * src/pfgt/pfgt.f:378-406.  bs0/cen0 are outputs in free space (iperiod=0)
+ * and inputs when periodic (src/common/pts_tree_nd.f:1350-1360).
+ */
+#ifndef FGT_B200_H
+#define FGT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FGT_OK 0
+#define FGT_ERR_ARG 1         /* invalid argument */
+#define FGT_ERR_CUDA 2        /* CUDA runtime error */
+#define FGT_ERR_NOMEM 3       /* device or host allocation failed */
+#define FGT_ERR_UNSUPPORTED 4 /* valid input outside the supported range */
+#define FGT_ERR_TIMEOUT 5     /* a bounded device wait gave up */
+#define FGT_ERR_NODEVICE 6    /* no CUDA device / library not usable */
+#define FGT_ERR_INJECTED 7    /* host-side fault injection (FGT_FAULT) */
+
+/* precision policy */
+#define FGT_PREC_AUTO 0  /* mixed FP32 bulk when eps >= 1e-6, FP64 otherwise */
+#define FGT_PREC_FP64 1  /* whole pipeline in FP64 */
+#define FGT_PREC_MIXED 2 /* FP32 bulk with FP64 geometry and accumulation */
+
+/* per-call statistics (filled when fgt_opts.stats != NULL) */
+typedef struct fgt_stats {
+  int nlevels, nboxes, npwlevel, npw, ndiv;
+  int precision_used;    /* FGT_PREC_FP64 or FGT_PREC_MIXED */
+  int n_form_boxes;      /* boxes that form a plane-wave expansion */
+  int n_eval_boxes;      /* boxes with a local plane-wave expansion */
+  int n_eval_nufft;      /* ... evaluated through the interpolation grid */
+  int n_translations;    /* sum over boxes of the PW list length */
+  int spread_width;      /* kernel width of the spreader */
+  int grid_cells;        /* spreading sub-grid cells per dimension */
+  int n_kernel_launches; /* kernels launched by this call */
+  double near_pairs;     /* source/target pairs of the direct near field */
+  double bs0, cen0[3];
+  /* milliseconds on the device stream: 0 h2d, 1 tree, 2 sort+gather,
+   * 3 lists, 4 form, 5 translate, 6 eval, 7 direct, 8 scatter, 9 d2h,
+   * 10 total */
+  double ms[12];
+} fgt_stats;
+
+typedef struct fgt_opts {
+  int precision;    /* FGT_PREC_* */
+  int device_ptrs;  /* 1: every array argument is a device pointer on `device` */
+  int device;       /* CUDA device ordinal, -1 = current device */
+  void *stream;     /* cudaStream_t to run on; NULL = the library's stream */
+  int ndiv;         /* max sources per unrefined box; 0 = reference value
+                       20/80/250 for dim 1/2/3 (src/pfgt/pfgt.f:122-128) */
+  int small_eval;   /* boxes with at most this many evaluation points use
+                       direct modal evaluation; -1 = tuned default */
+  int spread_width; /* spreading kernel width in grid cells; 0 = from eps */
+  int timing;       /* 1: record per-phase times into stats->ms */
+  fgt_stats *stats; /* optional output */
+} fgt_opts;
+
+/* Fill *opts with defaults (precision AUTO, host pointers, current device). */
+void fgt_opts_default(fgt_opts *opts);
+
+/*
+ * Point FGT with status return.  Same arguments and semantics as the
+ * reference pfgt (src/pfgt/pfgt.f:6-409) passed by value/pointer, plus the
+ * options pointer (NULL = defaults).  Returns FGT_OK or an FGT_ERR_* code.
+ */
+int fgt_pfgt_c(const fgt_opts *opts, int nd, int dim, double delta, double eps,
+               int iperiod, double *bs0, double *cen0, int ns,
+               const double *sources, int ifcharge, const double *charge,
+               int ifdipole, const double *rnormal, const double *dipstr,
+               int ifpgh, double *pot, double *grad, double *hess, int nt,
+               const double *targ, int ifpghtarg, double *pottarg,
+               double *gradtarg, double *hesstarg);
+
+/*
+ * gfortran-mangled drop-in for `call pfgt(...)` (src/pfgt/pfgt.f:6-10): all
+ * 24 arguments by reference, no hidden string lengths.  The reference has no
+ * error argument; on failure the requested outputs are NaN-filled and the
+ * status is kept for fgt_last_status().
+ */
+void pfgt_(const int *nd, const int *dim, const double *delta,
+           const double *eps, const int *iperiod, double *bs0, double *cen0,
+           const int *ns, const double *sources, const int *ifcharge,
+           const double *charge, const int *ifdipole, const double *rnormal,
+           const double *dipstr, const int *ifpgh, double *pot, double *grad,
+           double *hess, const int *nt, const double *targ,
+           const int *ifpghtarg, double *pottarg, double *gradtarg,
+           double *hesstarg);
+
+/*
+ * gfortran-mangled drop-in for `call pfgt_direct(...)` (src/pfgt/pfgt.f:
+ * 1156-1159): adds the direct Gaussian interactions of sources
+ * istart..iend onto targets jstart..jend (1-based, inclusive), cut off at
+ * squared distance dmax; periodic (iperiod=1) shifts the sources by
+ * shifts(dim).  Computed on the GPU in FP64.  Outputs are incremented.
+ */
+void pfgt_direct_(const int *nd, const int *dim, const double *delta,
+                  const double *dmax, const int *iperiod, const double *shifts,
+                  const int *istart, const int *iend, const int *jstart,
+                  const int *jend, const double *source, const int *ifcharge,
+                  const double *charge, const int *ifdipole,
+                  const double *rnormal, const double *dipstr,
+                  const double *targ, const int *ifpgh, double *pot,
+                  double *grad, double *hess);
+
+/* Status of the last pfgt_/pfgt_direct_ call on this host thread. */
+int fgt_last_status(void);
+
+/* Human-readable message of the last error on this host thread. */
+const char *fgt_last_error(void);
+
+/* Library version string. */
+const char *fgt_version(void);
+
+/*
+ * Introspection of the device-built tree and interaction lists (test and
+ * debugging support).  Builds the tree and lists of a pfgt call with the
+ * given arguments (host pointers) and keeps a host copy.  Returns NULL when
+ * no device is usable.  The tree replaces pts_tree_mem/pts_tree_build/
+ * pts_tree_sort (src/common/pts_tree_nd.f:35-644, 1226-1256); the lists
+ * replace pfgt_find_pwexp_boxes, pfgt_compute_listpw and
+ * pfgt_compute_modified_list1 (src/common/tree_routs_nd.f:1063-1555).
+ * Box ids are 0-based in level-major order, keys ascending within a level.
+ */
+void *fgt_debug_tree_build(int dim, double delta, double eps, int iperiod,
+                           double bs0, const double *cen0, int ns,
+                           const double *sources, int nt, const double *targ,
+                           int ndiv);
+/* Copies array `name` (see fgt_b200/__init__.py for the list) into dst
+ * (at most cap elements) and returns its length; dst may be NULL. */
+long fgt_debug_tree_get(void *h, const char *name, void *dst, long cap);
+void fgt_debug_tree_free(void *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FGT_B200_H */
