@@ -1,0 +1,392 @@
+"""Benchmark of the B200 point FGT (pfgt) on the headline workload.
+
+Workload: 3D, N = M = 1e7 points (sources = targets), 99% on the sphere of
+radius 0.4 plus 1% uniform background, charges N(0,1), delta = 1e-4,
+eps = 1e-6, potential + gradient at sources and targets (the delta=1e-4 cell
+of the precision sweep).  A step is one pfgt call over the whole point set.
+Metric: (N + M) evaluation points per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
+  python bench.py --impl reference   (CPU arm: the oracle port on host cores)
+
+Multi-GPU (torchrun): every rank runs an independent replica of the workload
+(weak scaling, no data-path collective); the timed region is bracketed by
+barriers and the max over ranks is reported.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "(N+M) pts/s, 3D N=1e7 eps=1e-6: mixed vs FP64 GPU path; rel err vs FP64 oracle"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="fgt", choices=["fgt", "reference"])
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    p.add_argument("--scale", type=float, default=1.0, help="fraction of N (tests only)")
+    p.add_argument("--delta", type=float, default=1e-4)
+    p.add_argument("--eps", type=float, default=1e-6)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-accuracy", action="store_true")
+    p.add_argument("--profile-once", action="store_true",
+                   help="one untimed step only (for ncu launch lists)")
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1].split()[0]))
+                smax.append(float(f[2].split()[0]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+_PEAK_CACHE = {}
+
+
+def flop_peak(dtype):
+    """Measured SIMT peak: cuBLAS GEMM of the kernel's arithmetic type
+    (TF32 off), best of 5 (TFLOP/s)."""
+    import torch
+    if dtype in _PEAK_CACHE:
+        return _PEAK_CACHE[dtype]
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192 if dtype == torch.float32 else 4096
+    x = torch.randn(n, n, dtype=dtype, device="cuda")
+    y = torch.randn(n, n, dtype=dtype, device="cuda")
+    for _ in range(2):
+        x @ y
+    best = 1e30
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        x @ y
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    v = 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    _PEAK_CACHE[dtype] = v
+    return v
+
+
+def ncu_traffic():
+    """Per-launch DRAM traffic of the dominant kernels from the committed ncu
+    summary (profiles/ncu_traffic.json), if present."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def roofline(a, stats, ms_phase):
+    """Roofline of the dominant phase (measured with CUDA events on the
+    launching stream inside the timed region)."""
+    import torch
+    names = {4: "form", 5: "translate", 6: "eval", 7: "direct"}
+    flops = {4: stats["flops_form"], 6: stats["flops_eval"], 7: stats["flops_direct"]}
+    dom = max(names, key=lambda i: ms_phase[i])
+    ms = float(ms_phase[dom])
+    tr = ncu_traffic().get(names[dom] + ("_" + a.precision), None)
+    if dom == 5:
+        bw, src = peaks()
+        ach = stats["bytes_translate"] / (ms * 1e-3) / 1e9
+        return {"bound": "hbm", "kernel": names[dom], "achieved": ach, "peak": bw,
+                "unit": "GB/s", "frac": ach / bw, "traffic": tr, "peak_source": src,
+                "ms": ms}
+    dt = torch.float32 if a.precision == "mixed" else torch.float64
+    pk = flop_peak(dt)
+    ach = flops[dom] / (ms * 1e-3) / 1e12
+    return {"bound": "fp32" if a.precision == "mixed" else "fp64", "kernel": names[dom],
+            "achieved": ach, "peak": pk, "unit": "TFLOP/s", "frac": ach / pk, "traffic": tr,
+            "peak_source": "measured cuBLAS %s GEMM in bench.py (no tensor-core path: "
+                           "no step is a dense contraction)" % ("FP32" if dt == torch.float32 else "FP64"),
+            "ms": ms, "flops": flops[dom]}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def sample_window(src, frac, rng):
+    """Points of the workload inside a cube around a sphere point holding
+    about `frac` of them: same local density and tree structure, bounded
+    size (the CPU baseline's sample)."""
+    n = src.shape[0]
+    c = src[rng.integers(n)]
+    d = np.max(np.abs(src - c), axis=1)
+    k = max(1000, int(frac * n))
+    h = np.partition(d, k)[k]
+    return np.nonzero(d <= h)[0]
+
+
+def cpu_reference(cfg, target_s=10.0, frac=None):
+    """Time the CPU restatement of the reference (FP64 C, OpenMP over boxes,
+    its own ES-kernel NUFFT) on a spatial window of the workload, grown until
+    one run takes about target_s; returns (pts/s, sample description, cores,
+    frac used)."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(1)
+    src = cfg["sources"]
+    frac = frac or 1e-3
+    while True:
+        idx = sample_window(src, frac, rng)
+        s = src[idx]
+        q = cfg["charge"][idx]
+        t0 = time.perf_counter()
+        O.pfgt(cfg["nd"], 3, cfg["delta"], cfg["eps"], 0, s, charge=q, ifpgh=cfg["ifpgh"],
+               targets=s.copy(), ifpghtarg=cfg["ifpghtarg"], nufft="spread")
+        t = time.perf_counter() - t0
+        if t >= 0.3 * target_s or frac >= 0.05:
+            break
+        frac = min(0.05, frac * max(2.0, min(8.0, target_s / max(t, 1e-3))))
+    npts = 2 * len(idx)
+    desc = (f"{len(idx)} sources + {len(idx)} targets (same points) inside a cube of the "
+            f"workload, {t:.2f} s per run, nufft=spread")
+    return npts / t, desc, O.threads(), frac
+
+
+def main():
+    a = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from fgt_b200 import workloads as W
+    cfg = W.config(5, scale=a.scale, delta=a.delta, eps=a.eps)
+    npts = cfg["sources"].shape[0] + cfg["targets"].shape[0]
+    config = {"workload": cfg["name"], "N": cfg["sources"].shape[0], "M": cfg["targets"].shape[0],
+              "delta": cfg["delta"], "eps": cfg["eps"], "dim": 3, "nd": 1,
+              "ifpgh": 2, "ifpghtarg": 2, "precision": a.precision,
+              "l2": "inputs larger than L2 (240 MB coordinates per side)"}
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        t0 = time.perf_counter()
+        vals = []
+        sample = ""
+        cores = 1
+        frac = None
+        for i in range(a.warmup + a.steps):
+            v, sample, cores, frac = cpu_reference(cfg, target_s=6.0, frac=frac)
+            if i >= a.warmup:
+                vals.append(v)
+        v = float(np.median(vals))
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "pts/s",
+                "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+                "ms_per_step": 1e3 * npts / v, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config,
+                "cpu_baseline": {"value": v, "unit": "pts/s", "cores": cores, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "pts/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "note": "reference Fortran build unavailable on this box (no Fortran "
+                        "compiler, finufft, FFTW); the timed CPU code is the C restatement"}
+        print(json.dumps(line))
+        return
+
+    import torch
+    import fgt_b200 as F
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    stream = torch.cuda.current_stream()
+    prec = F.PREC_MIXED if a.precision == "mixed" else F.PREC_FP64
+
+    # device-resident inputs and outputs (reference layouts, FP64)
+    src_d = torch.from_numpy(cfg["sources"]).to(dev)
+    trg_d = torch.from_numpy(cfg["targets"]).to(dev)
+    q_d = torch.from_numpy(cfg["charge"]).to(dev)
+    N, M = src_d.shape[0], trg_d.shape[0]
+    pot_d = torch.empty((N, 1), dtype=torch.float64, device=dev)
+    grad_d = torch.empty((N, 3, 1), dtype=torch.float64, device=dev)
+    pt_d = torch.empty((M, 1), dtype=torch.float64, device=dev)
+    gt_d = torch.empty((M, 3, 1), dtype=torch.float64, device=dev)
+    st = F.FgtStats()
+    import ctypes as C
+
+    def opts(device_ptrs, timing):
+        o = F.FgtOpts()
+        F.lib().fgt_opts_default(C.byref(o))
+        o.precision = prec
+        o.device_ptrs = device_ptrs
+        o.device = local
+        o.stream = C.c_void_p(stream.cuda_stream)
+        o.timing = 1 if timing else 0
+        o.stats = C.pointer(st)
+        return o
+
+    od = opts(1, True)
+
+    def step_dev():
+        F.pfgt_device(od, 1, 3, cfg["delta"], cfg["eps"], 0, 1.0, [0, 0, 0], N,
+                      src_d.data_ptr(), 1, q_d.data_ptr(), 0, None, None, 2,
+                      pot_d.data_ptr(), grad_d.data_ptr(), None, M, trg_d.data_ptr(), 2,
+                      pt_d.data_ptr(), gt_d.data_ptr(), None)
+
+    if a.profile_once:
+        step_dev()
+        torch.cuda.synchronize()
+        return
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def maxr(x):
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([x], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    for _ in range(a.warmup):
+        step_dev()
+    ms_phase = np.zeros(12)
+    barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        step_dev()
+        ms_phase += np.array(st.ms[:12])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier()
+    ms = maxr(e0.elapsed_time(e1) / a.steps)
+    ms_phase /= a.steps
+    stats = st.as_dict()
+    value = world * npts / (ms * 1e-3)
+
+    # end to end through the public API with pinned host buffers
+    e2e = None
+    if not a.no_e2e:
+        hs = torch.from_numpy(cfg["sources"]).pin_memory()
+        ht = torch.from_numpy(cfg["targets"]).pin_memory()
+        hq = torch.from_numpy(cfg["charge"]).pin_memory()
+        hp = torch.empty((N, 1), dtype=torch.float64).pin_memory()
+        hg = torch.empty((N, 3, 1), dtype=torch.float64).pin_memory()
+        hpt = torch.empty((M, 1), dtype=torch.float64).pin_memory()
+        hgt = torch.empty((M, 3, 1), dtype=torch.float64).pin_memory()
+        oh = opts(0, False)
+
+        def step_host():
+            F.pfgt_device(oh, 1, 3, cfg["delta"], cfg["eps"], 0, 1.0, [0, 0, 0], N,
+                          hs.data_ptr(), 1, hq.data_ptr(), 0, None, None, 2, hp.data_ptr(),
+                          hg.data_ptr(), None, M, ht.data_ptr(), 2, hpt.data_ptr(),
+                          hgt.data_ptr(), None)
+
+        for _ in range(max(1, a.warmup // 2)):
+            step_host()
+        barrier()
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(a.steps):
+            step_host()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms_e2e = maxr(f0.elapsed_time(f1) / a.steps)
+        h2d = (N * 3 + M * 3 + N) * 8
+        d2h = (N * 4 + M * 4) * 8
+        e2e = {"value": world * npts / (ms_e2e * 1e-3), "unit": "pts/s",
+               "ms_per_step": ms_e2e, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+
+    roof = roofline(a, stats, ms_phase)
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        v, desc, cores, _ = cpu_reference(cfg, target_s=12.0)
+        cpu = {"value": v, "unit": "pts/s", "cores": cores, "kind": "port", "sample": desc}
+    line = {"metric": METRIC, "value": value, "unit": "pts/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if a.precision == "mixed" else "f64", "data": "synthetic",
+            "config": config, "clocks": clocks, "e2e": e2e, "roofline": roof,
+            "cpu_baseline": cpu,
+            "gpu_launches": int(stats["n_kernel_launches"]) * a.steps,
+            "phases_ms": {k: round(float(v), 4) for k, v in zip(
+                ["h2d", "tree", "sort_gather", "lists", "form", "translate", "eval", "direct",
+                 "scatter", "d2h", "total"], ms_phase[:11])},
+            "stats": {k: stats[k] for k in ("nlevels", "nboxes", "npwlevel", "npw",
+                                             "n_form_boxes", "n_eval_boxes", "n_eval_nufft",
+                                             "n_translations", "spread_width", "grid_cells",
+                                             "near_pairs", "pts_form", "pts_eval_nufft",
+                                             "pts_eval_modal", "flops_form", "flops_eval",
+                                             "flops_direct", "bytes_translate")}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

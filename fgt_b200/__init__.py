@@ -42,7 +42,10 @@ class FgtStats(C.Structure):
         ("ndiv", C.c_int), ("precision_used", C.c_int), ("n_form_boxes", C.c_int),
         ("n_eval_boxes", C.c_int), ("n_eval_nufft", C.c_int), ("n_translations", C.c_int),
         ("spread_width", C.c_int), ("grid_cells", C.c_int), ("n_kernel_launches", C.c_int),
-        ("near_pairs", C.c_double), ("bs0", C.c_double), ("cen0", C.c_double * 3),
+        ("near_pairs", C.c_double), ("flops_form", C.c_double), ("flops_eval", C.c_double),
+        ("flops_direct", C.c_double), ("bytes_translate", C.c_double),
+        ("pts_form", C.c_double), ("pts_eval_nufft", C.c_double),
+        ("pts_eval_modal", C.c_double), ("bs0", C.c_double), ("cen0", C.c_double * 3),
         ("ms", C.c_double * 12),
     ]
 

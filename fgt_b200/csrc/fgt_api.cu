@@ -203,14 +203,14 @@ void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
   launches += do_pw ? 8 : 2;
   tm.mark(3);
   // --- gather (dreorderf, fmmcommon2d.f:3-27) as offsets from reference boxes
-  DBuf<T> soff((size_t)c.ns * dim, s), toff((size_t)std::max(c.nt, 1) * dim, s);
+  DBuf<double> soff((size_t)c.ns * dim, s), toff((size_t)std::max(c.nt, 1) * dim, s);
   DBuf<T> qs, dss, rns;
-  k_gather_coords<T><<<grid_for(c.ns, 256), 256, 0, s>>>(c.src, c.ns, dim, t.isrc, t.src_ref,
+  k_gather_coords<double><<<grid_for(c.ns, 256), 256, 0, s>>>(c.src, c.ns, dim, t.isrc, t.src_ref,
                                                           t.center, soff);
   FGT_LAUNCH_CHECK();
   launches++;
   if (c.nt > 0) {
-    k_gather_coords<T><<<grid_for(c.nt, 256), 256, 0, s>>>(c.trg, c.nt, dim, t.itrg, t.trg_ref,
+    k_gather_coords<double><<<grid_for(c.nt, 256), 256, 0, s>>>(c.trg, c.nt, dim, t.itrg, t.trg_ref,
                                                             t.center, toff);
     FGT_LAUNCH_CHECK();
     launches++;
@@ -252,18 +252,19 @@ void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
   et.n = c.nt; et.pgh = c.ifpghtarg; et.off = toff; et.lo = t.trg_lo; et.hi = t.trg_hi; et.out = outt;
   tm.mark(2);
   // --- plane waves (pfgt.f:700-1073)
-  int n_nufft = 0;
+  PWWork work;
   if (do_pw && L.n_eval > 0) {
     PWParams P;
     pw_setup(P, dim, nd, npw, pmax, periodic_nodes ? 1 : 0, t.boxsize[0], c.delta, c.eps,
              t.boxsize[t.ncutoff], o.spread_width);
     PWData<T> D;
-    launches += pw_form<T>(P, t, L, src, D, s);
+    PWWork* wk = st ? &work : nullptr;
+    launches += pw_form<T>(P, t, L, src, D, wk, s);
     tm.mark(4);
-    launches += pw_translate<T>(P, L, D, s);
+    launches += pw_translate<T>(P, L, D, wk, s);
     tm.mark(5);
     int se = o.small_eval >= 0 ? o.small_eval : -1;
-    launches += pw_eval<T>(P, t, L, D, es, et, se, &n_nufft, s);
+    launches += pw_eval<T>(P, t, L, D, es, et, se, wk, s);
     tm.mark(6);
     if (st) {
       st->spread_width = P.w;
@@ -306,7 +307,22 @@ void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
     st->ndiv = ndiv;
     st->n_form_boxes = L.n_form;
     st->n_eval_boxes = L.n_eval;
-    st->n_eval_nufft = n_nufft;
+    st->n_eval_nufft = work.n_nufft;
+    st->flops_form = work.flops_form;
+    st->flops_eval = work.flops_eval;
+    st->bytes_translate = work.bytes_translate;
+    st->pts_form = work.pts_form;
+    st->pts_eval_nufft = work.pts_nufft;
+    st->pts_eval_modal = work.pts_modal;
+    {
+      // near-field pair arithmetic (charge: 12 pot, 21 +grad, 21+5*nhess +hess)
+      auto per = [&](int pgh) {
+        double f = pgh >= 3 ? 21 + 5.0 * nhess : (pgh == 2 ? 21 : 12);
+        if (c.ifdipole) f += 4.0 * dim + 4;
+        return f;
+      };
+      st->flops_direct = pairs * per(std::max(c.ifpgh, c.ifpghtarg));
+    }
     st->n_translations = L.n_trans;
     st->near_pairs = pairs;
     st->n_kernel_launches = launches;
@@ -364,6 +380,7 @@ int pfgt_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps
   FGT_CUDA(cudaSetDevice(dev));
   configure_pool(dev);
   cudaStream_t s = o.stream ? (cudaStream_t)o.stream : library_stream(dev);
+  ArenaScope arena_scope(s);
   fgt_stats local_stats;
   fgt_stats* st = o.stats ? o.stats : nullptr;
   if (st) memset(st, 0, sizeof(*st));
@@ -525,6 +542,7 @@ extern "C" void* fgt_debug_tree_build(int dim, double delta, double eps, int ipe
     FGT_CUDA(cudaGetDevice(&dev));
     configure_pool(dev);
     cudaStream_t s = library_stream(dev);
+    ArenaScope arena_scope(s);
     DBuf<double> dsrc((size_t)ns * dim, s), dtrg((size_t)std::max(nt, 1) * dim, s);
     FGT_CUDA(cudaMemcpyAsync(dsrc.get(), src, sizeof(double) * ns * dim, cudaMemcpyHostToDevice, s));
     if (nt > 0)
@@ -623,6 +641,7 @@ extern "C" void pfgt_direct_(const int* nd, const int* dim, const double* delta,
       FGT_CUDA(cudaGetDevice(&dev));
       configure_pool(dev);
       cudaStream_t s = library_stream(dev);
+      ArenaScope arena_scope(s);
       auto up = [&](DBuf<double>& b, const double* h, size_t cnt) {
         b.alloc(cnt, s);
         FGT_CUDA(cudaMemcpyAsync(b.get(), h, sizeof(double) * cnt, cudaMemcpyHostToDevice, s));

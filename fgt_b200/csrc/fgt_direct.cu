@@ -21,7 +21,8 @@ struct DArgs {
   const int *item_box, *item_lo;
   const int *l1_ptr, *l1_src;
   const int *s_lo, *s_hi, *e_hi;
-  const T *soff, *q, *ds, *rn, *eoff;
+  const double *soff, *eoff;
+  const T *q, *ds, *rn;
   const double* center;
   double* out;
 };
@@ -48,7 +49,9 @@ template <typename T, int DIM, int PGH, bool CHG, bool DIP, int NDC>
 __global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
   constexpr int NH = DIM * (DIM + 1) / 2;
   constexpr int NC = 1 + (PGH >= 2 ? DIM : 0) + (PGH >= 3 ? NH : 0);
+  constexpr bool SPLIT = sizeof(T) == 4;  // FP32: pair differences from hi/lo parts
   __shared__ T sx[DW][DIM][32];
+  __shared__ T sxl[DW][SPLIT ? DIM : 1][32];
   __shared__ T sq[DW][CHG ? NDC : 1][32];
   __shared__ T sd[DW][DIP ? NDC : 1][32];
   __shared__ T sn[DW][DIP ? DIM : 1][32];
@@ -58,20 +61,29 @@ __global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
     const int tb = a.item_box[it];
     const int p = a.item_lo[it] + lane;
     const bool act = p < a.e_hi[tb];
-    T tx[DIM];
+    T tx[DIM], txl[DIM];
 #pragma unroll
-    for (int k = 0; k < DIM; k++) tx[k] = act ? a.eoff[(size_t)k * a.ne + p] : T(0);
+    for (int k = 0; k < DIM; k++) {
+      const double v = act ? a.eoff[(size_t)k * a.ne + p] : 0.0;
+      tx[k] = (T)v;
+      txl[k] = SPLIT ? (T)(v - (double)tx[k]) : T(0);
+    }
+    // T sums over one staged batch of 32 sources, FP64 sums over batches
     T acc[NDC][NC];
+    double accd[NDC][NC];
 #pragma unroll
     for (int i = 0; i < NDC; i++)
 #pragma unroll
-      for (int c = 0; c < NC; c++) acc[i][c] = T(0);
+      for (int c = 0; c < NC; c++) {
+        acc[i][c] = T(0);
+        accd[i][c] = 0.0;
+      }
     double cT[DIM];
 #pragma unroll
     for (int k = 0; k < DIM; k++) cT[k] = a.center[(size_t)tb * DIM + k];
     for (int li = a.l1_ptr[tb]; li < a.l1_ptr[tb + 1]; li++) {
       const int sb = a.l1_src[li];
-      T dc[DIM];
+      double dc[DIM];
 #pragma unroll
       for (int k = 0; k < DIM; k++) {
         double cs = a.center[(size_t)sb * DIM + k];
@@ -81,7 +93,7 @@ __global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
           if (fabs(dx) > fabs(dxp1)) { dx = dxp1; sh = a.bs0; }
           if (fabs(dx) > fabs(dxm1)) sh = -a.bs0;
         }
-        dc[k] = (T)((cs + sh) - cT[k]);
+        dc[k] = (cs + sh) - cT[k];
       }
       const int s0 = a.s_lo[sb], s1 = a.s_hi[sb];
       for (int base = s0; base < s1; base += 32) {
@@ -89,7 +101,12 @@ __global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
         __syncwarp();
         if (j < s1) {
 #pragma unroll
-          for (int k = 0; k < DIM; k++) sx[warp][k][lane] = a.soff[(size_t)k * a.ns + j] + dc[k];
+          for (int k = 0; k < DIM; k++) {
+            const double v = a.soff[(size_t)k * a.ns + j] + dc[k];
+            const T hi = (T)v;
+            sx[warp][k][lane] = hi;
+            if (SPLIT) sxl[warp][k][lane] = (T)(v - (double)hi);
+          }
           if (CHG)
 #pragma unroll
             for (int i = 0; i < NDC; i++)
@@ -104,11 +121,13 @@ __global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
         }
         __syncwarp();
         const int cnt = min(32, s1 - base);
+#pragma unroll 1
         for (int jj = 0; jj < cnt; jj++) {
           T dr[DIM], rr = T(0);
 #pragma unroll
           for (int k = 0; k < DIM; k++) {
-            dr[k] = tx[k] - sx[warp][k][jj];
+            dr[k] = SPLIT ? (tx[k] - sx[warp][k][jj]) + (txl[k] - sxl[warp][k][jj])
+                          : tx[k] - sx[warp][k][jj];
             rr += dr[k] * dr[k];
           }
           if (!(rr < a.dmax)) continue;
@@ -166,6 +185,13 @@ __global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
             }
           }
         }
+#pragma unroll
+        for (int i = 0; i < NDC; i++)
+#pragma unroll
+          for (int c = 0; c < NC; c++) {
+            accd[i][c] += (double)acc[i][c];
+            acc[i][c] = T(0);
+          }
       }
     }
     if (act) {
@@ -175,7 +201,7 @@ __global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
 #pragma unroll
         for (int c = 0; c < NC; c++) {
           double* o = &a.out[((size_t)c * a.nd + a.d0 + i) * a.ne + p];
-          *o += (double)acc[i][c];
+          *o += accd[i][c] + (double)acc[i][c];
         }
       }
     }
@@ -276,7 +302,7 @@ int direct_near_field(const DirectGeom& g, const Lists& L, const SourceSet<T>& s
   a.s_lo = src.lo;
   a.s_hi = src.hi;
   a.e_hi = e.hi;
-  a.soff = src.off;
+  a.soff = src.off;  // FP64
   a.q = src.q;
   a.ds = src.ds;
   a.rn = src.rn;

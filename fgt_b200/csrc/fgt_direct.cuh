@@ -9,7 +9,7 @@ template <typename T>
 struct EvalSet {
   int n = 0;                 // number of points
   int pgh = 0;               // 1 pot, 2 +grad, 3 +hess (0: nothing requested)
-  const T* off = nullptr;    // SoA [dim][n], offsets from the reference-box centre
+  const double* off = nullptr;  // SoA [dim][n], FP64 offsets from the reference-box centre
   const int* lo = nullptr;   // per box: first sorted index
   const int* hi = nullptr;   // per box: one past the last
   double* out = nullptr;     // SoA [(comp*nd + id)*n + i], comps pot,grad..,hess..
@@ -19,7 +19,7 @@ struct EvalSet {
 template <typename T>
 struct SourceSet {
   int n = 0;
-  const T* off = nullptr;  // [dim][n]
+  const double* off = nullptr;  // [dim][n], FP64 offsets from the box centre
   const T* q = nullptr;    // [nd][n] or null
   const T* ds = nullptr;   // [nd][n] or null (dipole strengths)
   const T* rn = nullptr;   // [dim][n] or null (dipole directions)

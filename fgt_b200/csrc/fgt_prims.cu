@@ -1,7 +1,66 @@
-// Scans, stable LSD radix sort and searches used by the tree build.
+// Workspace arena, scans, stable LSD radix sort and searches.
+#include <algorithm>
+#include <map>
+
 #include "fgt_prims.cuh"
 
 namespace fgt {
+
+void* Arena::alloc(size_t bytes) {
+  bytes = (bytes + 255) & ~size_t(255);
+  for (auto& c : chunks)
+    if (c.off + bytes <= c.cap) {
+      void* p = c.p + c.off;
+      c.off += bytes;
+      used += bytes;
+      high = std::max(high, used);
+      return p;
+    }
+  size_t cap = std::max(bytes, (size_t)256 << 20);
+  if (!chunks.empty()) cap = std::max(cap, chunks.back().cap);
+  char* p = nullptr;
+  if (cudaMalloc((void**)&p, cap) != cudaSuccess) {
+    (void)cudaGetLastError();
+    fgt_set_error_message("device workspace allocation failed", __FILE__, __LINE__);
+    throw Error{FGT_ERR_NOMEM, "device workspace allocation failed"};
+  }
+  chunks.push_back({p, cap, bytes});
+  used += bytes;
+  high = std::max(high, used);
+  return p;
+}
+
+void Arena::reset(cudaStream_t s) {
+  if (chunks.size() > 1) {
+    // consolidate into one chunk of the high-water size for the next call
+    cudaStreamSynchronize(s);
+    for (auto& c : chunks) cudaFree(c.p);
+    chunks.clear();
+    size_t cap = ((size_t)(high * 1.05) + ((size_t)1 << 20)) & ~(((size_t)1 << 20) - 1);
+    char* p = nullptr;
+    if (cudaMalloc((void**)&p, cap) == cudaSuccess) chunks.push_back({p, cap, 0});
+    else (void)cudaGetLastError();
+  }
+  for (auto& c : chunks) c.off = 0;
+  used = 0;
+}
+
+void Arena::release_all() {
+  for (auto& c : chunks) cudaFree(c.p);
+  chunks.clear();
+  used = high = 0;
+}
+
+Arena* thread_arena() {
+  static thread_local std::map<int, Arena*> arenas;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  auto it = arenas.find(dev);
+  if (it != arenas.end()) return it->second;
+  Arena* a = new Arena();
+  arenas[dev] = a;
+  return a;
+}
 
 namespace {
 

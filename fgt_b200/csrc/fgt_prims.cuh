@@ -1,11 +1,38 @@
 // Device primitives: stream-ordered buffers, scans, a stable LSD radix sort,
 // sorted-array searches.  All hand-written; no CUB/Thrust.
 #pragma once
+#include <vector>
+
 #include "fgt_common.cuh"
 
 namespace fgt {
 
-// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync).
+// Per-call device workspace: bump allocation from cached chunks that persist
+// across calls (reset at the end of every call; grown with cudaMalloc only
+// when a call needs more than any earlier one, then consolidated into one
+// chunk of the high-water size).  Removes allocation from the steady state.
+struct Arena {
+  struct Chunk {
+    char* p;
+    size_t cap, off;
+  };
+  std::vector<Chunk> chunks;
+  size_t used = 0, high = 0;
+  void* alloc(size_t bytes);
+  void reset(cudaStream_t s);  // call end: all allocations are dead
+  void release_all();
+};
+// Arena of the calling host thread on the current device (created lazily).
+Arena* thread_arena();
+// RAII scope of one library call: resets the arena on exit.
+struct ArenaScope {
+  Arena* a;
+  cudaStream_t s;
+  ArenaScope(cudaStream_t st) : a(thread_arena()), s(st) {}
+  ~ArenaScope() { a->reset(s); }
+};
+
+// Device buffer from the thread's arena (no per-call cudaMalloc).
 template <typename T>
 struct DBuf {
   T* p = nullptr;
@@ -29,19 +56,12 @@ struct DBuf {
     s = st;
     n = count;
     size_t bytes = (count ? count : 1) * sizeof(T);
-    cudaError_t e = cudaMallocAsync((void**)&p, bytes, st);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      (void)cudaGetLastError();
-      fgt_set_error_message("device allocation failed", __FILE__, __LINE__);
-      throw Error{FGT_ERR_NOMEM, "device allocation failed"};
-    }
+    p = (T*)thread_arena()->alloc(bytes);
   }
   void zero() {
     if (p) FGT_CUDA(cudaMemsetAsync(p, 0, (n ? n : 1) * sizeof(T), s));
   }
-  void release() {
-    if (p) cudaFreeAsync(p, s);
+  void release() {  // memory returns to the arena at the end of the call
     p = nullptr;
     n = 0;
   }

@@ -7,10 +7,13 @@
 // the pass that writes the expansion.  Only the sub-grid the box's points can
 // reach is stored: for boxes of the cut-off size the scaled coordinates lie
 // in [-pi/3, pi/3], about a third of the 2*pi period.
+//
+// Spreading and interpolation are thread-per-point over a bank-balanced
+// processing order of each box's points (see order_chunk), so the 32 lanes
+// of a warp touch 32 distinct shared-memory banks at every stencil offset.
 #include <math.h>
 
 #include <algorithm>
-#include <complex>
 #include <vector>
 
 #include "fgt_pw.cuh"
@@ -19,7 +22,9 @@ namespace fgt {
 
 namespace {
 
-constexpr int PW_THREADS = 256;
+constexpr int PW_THREADS = 512;
+constexpr int MODAL_THREADS = 256;
+constexpr int ORDER_CHUNK = 2048;  // points ordered per round (u16 indices)
 constexpr int MAXSMEM = 227 * 1024;
 
 struct Geo {
@@ -31,17 +36,27 @@ struct Geo {
 template <typename T>
 struct PWArgs {
   Geo g;
-  T scale, inv_dx, halfw_over_dx, beta, inv_halfw, dx, l0dx;
-  const T* twf;  // [G][2K+1] fwd full
-  const T* twh;  // [G][K+1]  fwd half
-  const T* tif;  // [2K+1][G] inv full
-  const T* tih;  // [K+1][G]  inv half (with 1/2/2/.. weights)
-  const T* facf; // [2K+1] dx*wsym/phihat
-  const T* faci; // [2K+1] dx/phihat
-  const T* ts;   // [2K+1] ts(k)
+  T halfw_over_dx, beta, dscale;
+  double scale_d, inv_dx_d, hwdx_d;  // FP64 positions (points are FP64 offsets)
+  const T* twf;   // [G][2K+1] fwd full
+  const T* twh;   // [G][K+1]  fwd half
+  const T* tif;   // [2K+1][G] inv full
+  const T* tih;   // [K+1][G]  inv half (with 1/2/2/.. weights)
+  const T* facf;  // [2K+1] dx*wsym/phihat
+  const T* faci;  // [2K+1] dx/phihat
+  const T* ts;    // [2K+1] ts(k)
   T inv_sqd0;
-  T* gscratch;   // global buffer slices when the grid does not fit in smem
+  T* gscratch;  // global buffer slices when the grid does not fit in smem
 };
+
+// byte offset of the grid buffer in shared memory: twiddles, then the
+// ordering scratch (ORDER_CHUNK ints + 32 counters + ORDER_CHUNK u16)
+template <typename T>
+__host__ __device__ constexpr size_t order_offset(int G, int K) {
+  return (((size_t)sizeof(T) * 2 * G * ((2 * K + 1) + (K + 1)) +
+           sizeof(int) * (ORDER_CHUNK + 32) + sizeof(unsigned short) * ORDER_CHUNK) + 15) &
+         ~(size_t)15;
+}
 
 // ---------------------------------------------------------------- passes
 // In-place line transforms over whole lines per round (a line is read
@@ -87,7 +102,6 @@ __device__ __forceinline__ void pass_inplace(T* B, int nl, int nb, int SA, int S
   }
 }
 
-// ES kernel value at offset t (grid units relative to the point).
 template <typename T>
 __device__ __forceinline__ T es_kernel(T z, T beta) {
   T u = T(1) - z * z;
@@ -95,125 +109,154 @@ __device__ __forceinline__ T es_kernel(T z, T beta) {
   return Real<T>::expm(beta * (T(1) - Real<T>::sqrt_(u)));
 }
 
-// First cell and kernel values of one coordinate.
-template <typename T, int W>
-__device__ __forceinline__ int kernel_row(const PWArgs<T>& a, T x, T* phi) {
-  // cells i0..i0+W-1 with i0 = ceil((x - halfw)/dx)
-  const T u = x * a.inv_dx;
-  const int i0 = (int)ceil(u - a.halfw_over_dx);
+__device__ __forceinline__ int pmod(int a, int n) {
+  int c = a % n;
+  return c < 0 ? c + n : c;
+}
+
+template <int DIM, int W>
+struct CellIdx {
+  int i0[DIM], base[DIM];
+  __device__ __forceinline__ void init(const Geo& g, const int* s) {
 #pragma unroll
-  for (int j = 0; j < W; j++) {
-    const T z = ((T)(i0 + j) - u) / a.halfw_over_dx;
-    phi[j] = es_kernel<T>(z, a.beta);
+    for (int d = 0; d < DIM; d++) {
+      i0[d] = s[d];
+      int b = s[d] - g.l0;
+      base[d] = b < 0 ? 0 : (b > g.G - W ? g.G - W : b);
+    }
   }
+  __device__ __forceinline__ int at(const Geo& g, int d, int j) const {
+    return g.wrap ? pmod(i0[d] + j, g.nf) : base[d] + j;
+  }
+};
+
+// Thread-per-point interpolation (component grids of the hessian path).
+template <typename T, int W>
+__device__ __forceinline__ int kernel_row(const PWArgs<T>& a, double x, T* phi) {
+  const double u = x * a.inv_dx_d;
+  const int i0 = (int)ceil(u - a.hwdx_d);
+  const T f0 = (T)((double)i0 - u);
+#pragma unroll
+  for (int j = 0; j < W; j++) phi[j] = es_kernel<T>((f0 + (T)j) / a.halfw_over_dx, a.beta);
   return i0;
 }
 
-template <typename T, int W>
-__device__ __forceinline__ void cell_index(const Geo& g, int i0, int* idx) {
-  // local cell indices (wrapped on the full periodic grid)
-  if (g.wrap) {
-#pragma unroll
-    for (int j = 0; j < W; j++) {
-      int c = (i0 + j) % g.nf;
-      idx[j] = c < 0 ? c + g.nf : c;
-    }
-  } else {
-    int b = i0 - g.l0;
-    b = b < 0 ? 0 : (b > g.G - W ? g.G - W : b);
-#pragma unroll
-    for (int j = 0; j < W; j++) idx[j] = b + j;
-  }
-}
-
 template <typename T, int DIM, int W>
-__device__ __forceinline__ void spread_point(const PWArgs<T>& a, T* B, const T* x, T str) {
+__device__ __forceinline__ T interp_point(const PWArgs<T>& a, const T* B, const double* x) {
   const Geo& g = a.g;
-  if (DIM == 1) {
-    T px[W];
-    int ix[W];
-    cell_index<T, W>(g, kernel_row<T, W>(a, x[0], px), ix);
+  T ph[DIM][W];
+  int s[DIM];
 #pragma unroll
-    for (int j = 0; j < W; j++) atomicAdd(&B[ix[j]], str * px[j]);
-  } else if (DIM == 2) {
-    T px[W], py[W];
-    int ix[W], iy[W];
-    cell_index<T, W>(g, kernel_row<T, W>(a, x[0], px), ix);
-    cell_index<T, W>(g, kernel_row<T, W>(a, x[1], py), iy);
-#pragma unroll 1
-    for (int jx = 0; jx < W; jx++) {
-      const T v = str * px[jx];
-      const int bx = ix[jx] * g.str[0];
-#pragma unroll
-      for (int jy = 0; jy < W; jy++) atomicAdd(&B[bx + iy[jy]], v * py[jy]);
-    }
-  } else {
-    T py[W], pz[W];
-    int ix[W], iy[W], iz[W];
-    T px[W];
-    cell_index<T, W>(g, kernel_row<T, W>(a, x[0], px), ix);
-    cell_index<T, W>(g, kernel_row<T, W>(a, x[1], py), iy);
-    cell_index<T, W>(g, kernel_row<T, W>(a, x[2], pz), iz);
-#pragma unroll 1
-    for (int jx = 0; jx < W; jx++) {
-      const T vx = str * px[jx];
-      const int bx = ix[jx] * g.str[0];
-#pragma unroll
-      for (int jy = 0; jy < W; jy++) {
-        const T vxy = vx * py[jy];
-        const int bxy = bx + iy[jy] * g.str[1];
-#pragma unroll
-        for (int jz = 0; jz < W; jz++) atomicAdd(&B[bxy + iz[jz]], vxy * pz[jz]);
-      }
-    }
-  }
-}
-
-template <typename T, int DIM, int W>
-__device__ __forceinline__ T interp_point(const PWArgs<T>& a, const T* B, const T* x) {
-  const Geo& g = a.g;
+  for (int d = 0; d < DIM; d++) s[d] = kernel_row<T, W>(a, x[d], ph[d]);
+  CellIdx<DIM, W> c;
+  c.init(g, s);
   T acc = T(0);
   if (DIM == 1) {
-    T px[W];
-    int ix[W];
-    cell_index<T, W>(g, kernel_row<T, W>(a, x[0], px), ix);
 #pragma unroll
-    for (int j = 0; j < W; j++) acc += B[ix[j]] * px[j];
+    for (int j = 0; j < W; j++) acc += B[c.at(g, 0, j)] * ph[0][j];
   } else if (DIM == 2) {
-    T px[W], py[W];
-    int ix[W], iy[W];
-    cell_index<T, W>(g, kernel_row<T, W>(a, x[0], px), ix);
-    cell_index<T, W>(g, kernel_row<T, W>(a, x[1], py), iy);
 #pragma unroll 1
     for (int jx = 0; jx < W; jx++) {
-      const int bx = ix[jx] * g.str[0];
-      T s = T(0);
+      const int bx = c.at(g, 0, jx) * g.str[0];
+      T sy = T(0);
 #pragma unroll
-      for (int jy = 0; jy < W; jy++) s += B[bx + iy[jy]] * py[jy];
-      acc += s * px[jx];
+      for (int jy = 0; jy < W; jy++) sy += B[bx + c.at(g, 1, jy)] * ph[1][jy];
+      acc += sy * ph[0][jx];
     }
   } else {
-    T px[W], py[W], pz[W];
-    int ix[W], iy[W], iz[W];
-    cell_index<T, W>(g, kernel_row<T, W>(a, x[0], px), ix);
-    cell_index<T, W>(g, kernel_row<T, W>(a, x[1], py), iy);
-    cell_index<T, W>(g, kernel_row<T, W>(a, x[2], pz), iz);
 #pragma unroll 1
     for (int jx = 0; jx < W; jx++) {
-      const int bx = ix[jx] * g.str[0];
+      const int bx = c.at(g, 0, jx) * g.str[0];
       T sx = T(0);
 #pragma unroll
       for (int jy = 0; jy < W; jy++) {
-        const int bxy = bx + iy[jy] * g.str[1];
+        const int bxy = bx + c.at(g, 1, jy) * g.str[1];
         T sy = T(0);
 #pragma unroll
-        for (int jz = 0; jz < W; jz++) sy += B[bxy + iz[jz]] * pz[jz];
-        sx += sy * py[jy];
+        for (int jz = 0; jz < W; jz++) sy += B[bxy + c.at(g, 2, jz)] * ph[2][jz];
+        sx += sy * ph[1][jy];
       }
-      acc += sx * px[jx];
+      acc += sx * ph[0][jx];
     }
   }
   return acc;
+}
+
+template <typename T, int DIM, int W>
+__device__ __forceinline__ void spread_point(const PWArgs<T>& a, T* B, const double* x, T str) {
+  const Geo& g = a.g;
+  T ph[DIM][W];
+  int s[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) s[d] = kernel_row<T, W>(a, x[d], ph[d]);
+  CellIdx<DIM, W> c;
+  c.init(g, s);
+  if (DIM == 1) {
+#pragma unroll
+    for (int j = 0; j < W; j++) atomicAdd(&B[c.at(g, 0, j)], str * ph[0][j]);
+  } else if (DIM == 2) {
+#pragma unroll 1
+    for (int jx = 0; jx < W; jx++) {
+      const int bx = c.at(g, 0, jx) * g.str[0];
+      const T v = str * ph[0][jx];
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) atomicAdd(&B[bx + c.at(g, 1, jy)], v * ph[1][jy]);
+    }
+  } else {
+#pragma unroll 1
+    for (int jx = 0; jx < W; jx++) {
+      const int bx = c.at(g, 0, jx) * g.str[0];
+      const T vx = str * ph[0][jx];
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        const int bxy = bx + c.at(g, 1, jy) * g.str[1];
+        const T vxy = vx * ph[1][jy];
+#pragma unroll
+        for (int jz = 0; jz < W; jz++) atomicAdd(&B[bxy + c.at(g, 2, jz)], vxy * ph[2][jz]);
+      }
+    }
+  }
+}
+
+// Bank-balanced processing order of a chunk of points.  Thread-per-point
+// stencils touch B[base_p + offset] for the same offset in every lane at
+// once; ordering the chunk by (rank within bank class, bank class) with
+// class = base_p mod NCLASS puts NCLASS different classes into every run of
+// NCLASS consecutive points, so those accesses hit distinct banks.
+template <typename T, int DIM, int W>
+__device__ __forceinline__ void order_chunk(const PWArgs<T>& a, const double* off, int ne, int q0,
+                                            int n, unsigned short* perm, int* tmp, int* cnt) {
+  constexpr int NCLASS = sizeof(T) == 4 ? 32 : 16;  // 4-byte banks
+  const Geo& g = a.g;
+  if (threadIdx.x < NCLASS) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int base = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const double u = off[(size_t)d * ne + q0 + i] * a.scale_d * a.inv_dx_d;
+      const int i0 = (int)ceil(u - a.hwdx_d);
+      int b = g.wrap ? pmod(i0, g.nf) : i0 - g.l0;
+      if (!g.wrap) b = b < 0 ? 0 : (b > g.G - W ? g.G - W : b);
+      base += b * g.str[d];
+    }
+    const int cls = base & (NCLASS - 1);
+    const int rank = atomicAdd(&cnt[cls], 1);
+    tmp[i] = rank * NCLASS + cls;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int rank = tmp[i] / NCLASS, cls = tmp[i] % NCLASS;
+    int pos = 0;
+#pragma unroll 8
+    for (int c = 0; c < NCLASS; c++) {
+      const int k = cnt[c];
+      pos += k < rank ? k : rank;
+      pos += (c < cls && k > rank) ? 1 : 0;
+    }
+    perm[pos] = (unsigned short)i;
+  }
+  __syncthreads();
 }
 
 template <typename T>
@@ -230,8 +273,9 @@ struct FormIO {
 
 template <typename T>
 struct FormPtrs {
-  const T *off, *q, *ds, *rn;  // sorted SoA
-  T* mp;                       // [n_form][nd][nexp] complex
+  const double* off;     // sorted SoA FP64 offsets
+  const T *q, *ds, *rn;  // sorted SoA
+  T* mp;                 // [n_form][nd][nexp] complex
 };
 
 template <typename T, int DIM, int W, bool GB>
@@ -240,9 +284,13 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
   const Geo& g = a.g;
   const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
   T* sm = reinterpret_cast<T*>(smem_raw);
-  T* twf = sm;                    // G*NF complex
-  T* twh = twf + 2 * G * NF;      // G*NH complex
-  T* B = GB ? a.gscratch + (size_t)blockIdx.x * g.bufsz : (twh + 2 * G * NH);
+  T* twf = sm;                // G*NF complex
+  T* twh = twf + 2 * G * NF;  // G*NH complex
+  int* ordtmp = reinterpret_cast<int*>(twh + 2 * G * NH);  // ORDER_CHUNK
+  int* ordcnt = ordtmp + ORDER_CHUNK;                        // 32
+  unsigned short* perm = reinterpret_cast<unsigned short*>(ordcnt + 32);  // ORDER_CHUNK
+  T* B = GB ? a.gscratch + (size_t)blockIdx.x * g.bufsz
+            : reinterpret_cast<T*>(smem_raw + order_offset<T>(G, K));
   load_tw(twf, a.twf, 2 * G * NF);
   load_tw(twh, a.twh, 2 * G * NH);
   __syncthreads();
@@ -258,15 +306,20 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
         const int dd = is_q ? -1 : comp - io.has_q;
         for (int i = threadIdx.x; i < g.bufsz; i += blockDim.x) B[i] = T(0);
         __syncthreads();
-        for (int pt = p0 + threadIdx.x; pt < p1; pt += blockDim.x) {
-          T x[DIM];
+        for (int c0 = p0; c0 < p1; c0 += ORDER_CHUNK) {
+          const int n = min(ORDER_CHUNK, p1 - c0);
+          order_chunk<T, DIM, W>(a, p.off, io.ns, c0, n, perm, ordtmp, ordcnt);
+          for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int pt = c0 + perm[i];
+            double x[DIM];
 #pragma unroll
-          for (int k = 0; k < DIM; k++) x[k] = p.off[(size_t)k * io.ns + pt] * a.scale;
-          T str = is_q ? p.q[(size_t)id * io.ns + pt]
-                       : p.ds[(size_t)id * io.ns + pt] * p.rn[(size_t)dd * io.ns + pt];
-          spread_point<T, DIM, W>(a, B, x, str);
+            for (int k = 0; k < DIM; k++) x[k] = p.off[(size_t)k * io.ns + pt] * a.scale_d;
+            const T str = is_q ? p.q[(size_t)id * io.ns + pt]
+                               : p.ds[(size_t)id * io.ns + pt] * p.rn[(size_t)dd * io.ns + pt];
+            spread_point<T, DIM, W>(a, B, x, str);
+          }
+          __syncthreads();
         }
-        __syncthreads();
         // passes on the last and middle dimensions
         if (DIM == 3) {
           pass_inplace<T, 0>(B, G * G, G, g.str[0], g.str[1], 1, 2, G, NH, twh);
@@ -305,7 +358,6 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
               im += xr * ti + xi * tr;
             }
           }
-          // mode indices (k+K) per dimension; last dim stored k = 0..K
           int ki[3];
           if (DIM == 3) { ki[0] = kxi; ki[1] = kyi; ki[2] = kz + K; }
           else if (DIM == 2) { ki[0] = kxi; ki[1] = kz + K; }
@@ -315,8 +367,8 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
           for (int d = 0; d < DIM; d++) f *= a.facf[ki[d]];
           T vr = re * f, vi = im * f;
           if (!is_q) {  // * (-i) ts(k_d) / sqrt(delta0)
-            const T c = a.ts[ki[dd]] * a.inv_sqd0;
-            const T tr = vi * c, ti = -vr * c;
+            const T cc = a.ts[ki[dd]] * a.inv_sqd0;
+            const T tr = vi * cc, ti = -vr * cc;
             vr = tr;
             vi = ti;
           }
@@ -394,12 +446,12 @@ __global__ void k_wtab(int dim, int K, int nexp, const double* __restrict__ ts, 
 // ---------------------------------------------------------------- eval
 template <typename T>
 struct EvalPtrs {
-  const T* loc;  // [n_eval][nd][nexp]
-  const int* boxes;   // eval slots handled by this launch
+  const T* loc;      // [n_eval][nd][nexp]
+  const int* boxes;  // eval slots handled by this launch
   const int* eval_box;
   int nbox;
   // two evaluation sets (sources, targets)
-  const T* off[2];
+  const double* off[2];
   const int* lo[2];
   const int* hi[2];
   double* out[2];
@@ -410,7 +462,11 @@ struct EvalPtrs {
 // component factor (complex) of evaluation component c at mode ki[]
 template <typename T, int DIM>
 __device__ __forceinline__ void eval_factor(const PWArgs<T>& a, int c, const int* ki, T& fr, T& fi) {
-  if (c == 0) { fr = T(1); fi = T(0); return; }
+  if (c == 0) {
+    fr = T(1);
+    fi = T(0);
+    return;
+  }
   if (c <= DIM) {  // i ts(k_d)/sqrt(delta0)
     fr = T(0);
     fi = a.ts[ki[c - 1]] * a.inv_sqd0;
@@ -424,15 +480,83 @@ __device__ __forceinline__ void eval_factor(const PWArgs<T>& a, int c, const int
   fi = T(0);
 }
 
+// Grid of evaluation component c of expansion L in buffer B (real values).
+template <typename T, int DIM>
+__device__ __forceinline__ void build_eval_grid(const PWArgs<T>& a, const T* L, int c, T* B,
+                                                const T* tif, const T* tih) {
+  const Geo& g = a.g;
+  const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
+  const int nline = DIM == 3 ? NF * NH : (DIM == 2 ? NH : 1);
+  if (DIM == 1) {
+    for (int l = threadIdx.x; l < G; l += blockDim.x) {
+      T acc = T(0);
+      for (int k = 0; k < NH; k++) {
+        int ki[1] = {k + K};
+        T fr, fi;
+        eval_factor<T, DIM>(a, c, ki, fr, fi);
+        const T f = a.faci[k + K];
+        const T lr = L[2 * k] * f, li = L[2 * k + 1] * f;
+        const T mr = lr * fr - li * fi, mi = lr * fi + li * fr;
+        acc += mr * tih[2 * (k * G + l)] - mi * tih[2 * (k * G + l) + 1];
+      }
+      B[l] = acc;
+    }
+    __syncthreads();
+    return;
+  }
+  // expansion times factors at B[kx][ky][kz], then the x pass in place
+  for (int m = threadIdx.x; m < g.nexp; m += blockDim.x) {
+    int ki[3], pos;
+    if (DIM == 3) {
+      const int kxi = m / nline, line = m - kxi * nline;
+      const int kyi = line / NH, kz = line - kyi * NH;
+      ki[0] = kxi;
+      ki[1] = kyi;
+      ki[2] = kz + K;
+      pos = kxi * g.str[0] + kyi * g.str[1] + 2 * kz;
+    } else {
+      const int kxi = m / NH, ky = m - kxi * NH;
+      ki[0] = kxi;
+      ki[1] = ky + K;
+      pos = kxi * g.str[0] + 2 * ky;
+    }
+    T f = T(1);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) f *= a.faci[ki[d]];
+    T fr, fi;
+    eval_factor<T, DIM>(a, c, ki, fr, fi);
+    fr *= f;
+    fi *= f;
+    const T lr = L[2 * m], li = L[2 * m + 1];
+    B[pos] = lr * fr - li * fi;
+    B[pos + 1] = lr * fi + li * fr;
+  }
+  __syncthreads();
+  if (DIM == 3) {
+    pass_inplace<T, 1>(B, NF * NH, NH, g.str[1], 2, g.str[0], g.str[0], NF, G, tif);
+    pass_inplace<T, 1>(B, G * NH, NH, g.str[0], 2, g.str[1], g.str[1], NF, G, tif);
+    pass_inplace<T, 2>(B, G * G, G, g.str[0], g.str[1], 2, 1, NH, G, tih);
+  } else {
+    pass_inplace<T, 1>(B, NH, 1, 2, 0, g.str[0], g.str[0], NF, G, tif);
+    pass_inplace<T, 2>(B, G, 1, g.str[0], 0, 2, 1, NH, G, tih);
+  }
+}
+
+// One grid per output component (pot, grad_k, hess_kl) and thread-per-point
+// interpolation of both evaluation sets in bank-balanced order.
 template <typename T, int DIM, int W, bool GB>
-__global__ void __launch_bounds__(PW_THREADS) k_eval_nufft(PWArgs<T> a, EvalPtrs<T> p) {
+__global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<T> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geo& g = a.g;
   const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
   T* sm = reinterpret_cast<T*>(smem_raw);
-  T* tif = sm;                 // NF*G complex
-  T* tih = tif + 2 * NF * G;   // NH*G complex
-  T* B = GB ? a.gscratch + (size_t)blockIdx.x * g.bufsz : (tih + 2 * NH * G);
+  T* tif = sm;
+  T* tih = tif + 2 * NF * G;
+  int* ordtmp = reinterpret_cast<int*>(tih + 2 * NH * G);
+  int* ordcnt = ordtmp + ORDER_CHUNK;
+  unsigned short* perm = reinterpret_cast<unsigned short*>(ordcnt + 32);
+  T* B = GB ? a.gscratch + (size_t)blockIdx.x * g.bufsz
+            : reinterpret_cast<T*>(smem_raw + order_offset<T>(G, K));
   load_tw(tif, a.tif, 2 * NF * G);
   load_tw(tih, a.tih, 2 * NH * G);
   __syncthreads();
@@ -442,73 +566,22 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_nufft(PWArgs<T> a, EvalPtrs
     for (int id = 0; id < p.nd; id++) {
       const T* L = p.loc + ((size_t)e * p.nd + id) * 2 * g.nexp;
       for (int c = 0; c < p.ncomp_max; c++) {
-        // first pass (x) from the expansion into the grid buffer
-        const int nline = DIM == 3 ? NF * NH : (DIM == 2 ? NH : 1);
-        if (DIM == 1) {
-          for (int l = threadIdx.x; l < G; l += blockDim.x) {
-            T acc = T(0);
-            for (int k = 0; k < NH; k++) {
-              int ki[1] = {k + K};
-              T fr, fi;
-              eval_factor<T, DIM>(a, c, ki, fr, fi);
-              const T f = a.faci[k + K];
-              const T lr = L[2 * k] * f, li = L[2 * k + 1] * f;
-              const T mr = lr * fr - li * fi, mi = lr * fi + li * fr;
-              acc += mr * tih[2 * (k * G + l)] - mi * tih[2 * (k * G + l) + 1];
-            }
-            B[l] = acc;
-          }
-        } else {
-          for (int o = threadIdx.x; o < G * nline; o += blockDim.x) {
-            const int ix = o / nline, line = o - ix * nline;
-            int ki[3], lb;
-            if (DIM == 3) {
-              const int kyi = line / NH, kz = line - kyi * NH;
-              ki[1] = kyi;
-              ki[2] = kz + K;
-              lb = kyi * g.str[1] + 2 * kz;
-            } else {
-              ki[1] = line + K;
-              lb = 2 * line;
-            }
-            T fyz = T(1);
-#pragma unroll
-            for (int d = 1; d < DIM; d++) fyz *= a.faci[ki[d]];
-            T re = T(0), im = T(0);
-            for (int kxi = 0; kxi < NF; kxi++) {
-              ki[0] = kxi;
-              T fr, fi;
-              eval_factor<T, DIM>(a, c, ki, fr, fi);
-              const T f = fyz * a.faci[kxi];
-              const int m = kxi * nline + line;
-              const T lr = L[2 * m] * f, li = L[2 * m + 1] * f;
-              const T mr = lr * fr - li * fi, mi = lr * fi + li * fr;
-              const T tr = tif[2 * (kxi * G + ix)], ti = tif[2 * (kxi * G + ix) + 1];
-              re += mr * tr - mi * ti;
-              im += mr * ti + mi * tr;
-            }
-            B[ix * g.str[0] + lb] = re;
-            B[ix * g.str[0] + lb + 1] = im;
-          }
-        }
-        __syncthreads();
-        if (DIM == 3) {
-          pass_inplace<T, 1>(B, G * NH, NH, g.str[0], 2, g.str[1], g.str[1], NF, G, tif);
-          pass_inplace<T, 2>(B, G * G, G, g.str[0], g.str[1], 2, 1, NH, G, tih);
-        } else if (DIM == 2) {
-          pass_inplace<T, 2>(B, G, 1, g.str[0], 0, 2, 1, NH, G, tih);
-        }
-        // interpolate at the points of both evaluation sets
+        build_eval_grid<T, DIM>(a, L, c, B, tif, tih);
         for (int set = 0; set < 2; set++) {
           if (c >= p.ncomp[set] || p.n[set] == 0) continue;
-          const int q0 = p.lo[set][box], q1 = p.hi[set][box];
-          const int ne = p.n[set];
-          for (int pt = q0 + threadIdx.x; pt < q1; pt += blockDim.x) {
-            T x[DIM];
+          const int q0 = p.lo[set][box], q1 = p.hi[set][box], ne = p.n[set];
+          for (int c0 = q0; c0 < q1; c0 += ORDER_CHUNK) {
+            const int n = min(ORDER_CHUNK, q1 - c0);
+            order_chunk<T, DIM, W>(a, p.off[set], ne, c0, n, perm, ordtmp, ordcnt);
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+              const int pt = c0 + perm[i];
+              double x[DIM];
 #pragma unroll
-            for (int k = 0; k < DIM; k++) x[k] = p.off[set][(size_t)k * ne + pt] * a.scale;
-            const T v = interp_point<T, DIM, W>(a, B, x);
-            p.out[set][((size_t)c * p.nd + id) * ne + pt] += (double)v;
+              for (int k = 0; k < DIM; k++) x[k] = p.off[set][(size_t)k * ne + pt] * a.scale_d;
+              const T v = interp_point<T, DIM, W>(a, B, x);
+              p.out[set][((size_t)c * p.nd + id) * ne + pt] += (double)v;
+            }
+            __syncthreads();
           }
         }
         __syncthreads();
@@ -517,19 +590,15 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_nufft(PWArgs<T> a, EvalPtrs
   }
 }
 
-__device__ __forceinline__ void sincos_(float x, float* s, float* c) { sincosf(x, s, c); }
-__device__ __forceinline__ void sincos_(double x, double* s, double* c) { sincos(x, s, c); }
-
 // Direct modal evaluation for boxes with few points: one CTA per box, modes
 // split over threads, one block reduction per point.
 template <typename T, int DIM>
-__global__ void __launch_bounds__(PW_THREADS) k_eval_modal(PWArgs<T> a, EvalPtrs<T> p) {
+__global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal(PWArgs<T> a, EvalPtrs<T> p) {
   const Geo& g = a.g;
   const int K = g.K, NF = 2 * K + 1, NH = K + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* E = reinterpret_cast<T*>(smem_raw);  // [DIM][NF] complex e^{i k x_d}
-  __shared__ double red[PW_THREADS / 32][10];
-  const int nl = DIM == 3 ? NF * NH : (DIM == 2 ? NH : 1);
+  __shared__ double red[MODAL_THREADS / 32][10];
   for (int bi = blockIdx.x; bi < p.nbox; bi += gridDim.x) {
     const int e = p.boxes[bi];
     const int box = p.eval_box[e];
@@ -540,11 +609,11 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_modal(PWArgs<T> a, EvalPtrs
         __syncthreads();
         for (int i = threadIdx.x; i < DIM * NF; i += blockDim.x) {
           const int d = i / NF, k = i - d * NF - K;
-          const T x = p.off[set][(size_t)d * ne + pt] * a.scale;
-          T sn, cs;
-          sincos_(x * (T)k, &sn, &cs);
-          E[2 * i] = cs;
-          E[2 * i + 1] = sn;
+          const double x = p.off[set][(size_t)d * ne + pt] * a.scale_d;
+          double sn, cs;
+          sincos(x * (double)k, &sn, &cs);
+          E[2 * i] = (T)cs;
+          E[2 * i + 1] = (T)sn;
         }
         __syncthreads();
         for (int id = 0; id < p.nd; id++) {
@@ -557,7 +626,7 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_modal(PWArgs<T> a, EvalPtrs
             if (DIM == 3) { ki[0] = m / (NF * NH); ki[1] = (m / NH) % NF; ki[2] = m % NH + K; }
             else if (DIM == 2) { ki[0] = m / NH; ki[1] = m % NH + K; }
             else { ki[0] = m + K; }
-            T f = (ki[DIM - 1] == K) ? T(1) : T(2);  // Hermitian half-space weight
+            const T f = (ki[DIM - 1] == K) ? T(1) : T(2);  // Hermitian half-space weight
             T er = T(1), ei = T(0);
 #pragma unroll
             for (int d = 0; d < DIM; d++) {
@@ -584,7 +653,6 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_modal(PWArgs<T> a, EvalPtrs
               }
             }
           }
-          // block reduction of nc values
           const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
           for (int c = 0; c < nc; c++) {
             double v = (double)acc[c];
@@ -607,12 +675,19 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_modal(PWArgs<T> a, EvalPtrs
 // box partition by evaluation-point count
 __global__ void k_eval_split(int n_eval, const int* __restrict__ eval_box, const int* __restrict__ lo0,
                              const int* __restrict__ hi0, const int* __restrict__ lo1,
-                             const int* __restrict__ hi1, int thr, int* __restrict__ big) {
+                             const int* __restrict__ hi1, int thr, int* __restrict__ big,
+                             unsigned long long* __restrict__ cnt) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_eval; e += gridDim.x * blockDim.x) {
     int b = eval_box[e];
     int n = (lo0 ? hi0[b] - lo0[b] : 0) + (lo1 ? hi1[b] - lo1[b] : 0);
     big[e] = n > thr ? 1 : 0;
+    atomicAdd(&cnt[n > thr ? 0 : 1], (unsigned long long)n);
   }
+}
+__global__ void k_count_points(int n, const int* __restrict__ box, const int* __restrict__ lo,
+                               const int* __restrict__ hi, unsigned long long* __restrict__ cnt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    atomicAdd(cnt, (unsigned long long)(hi[box[i]] - lo[box[i]]));
 }
 __global__ void k_split_fill(int n, const int* __restrict__ f, const int* __restrict__ pos,
                              int* __restrict__ big_list, int* __restrict__ small_list) {
@@ -632,11 +707,13 @@ int supported_w(int w) {
 template <typename T>
 struct DevTables {
   DBuf<T> twf, twh, tif, tih, facf, faci, ts;
-  DBuf<double> ts64;
 };
 
+// Device arguments for grid parameters P; the innermost buffer stride is
+// padded to W (mod 32) words for FP32 so the warp-per-point stencils are
+// bank-conflict free.
 template <typename T>
-void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s) {
+void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s, bool pad) {
   Geo& g = a.g;
   g.dim = P.dim;
   g.K = P.K;
@@ -658,18 +735,21 @@ void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s
   } else {
     S[0] = std::max(G, 2 * NH);
   }
+  if (pad && sizeof(T) == 4 && P.dim >= 2) {
+    int& last = S[P.dim - 1];
+    while ((last - P.w) % 32 != 0 || (last & 1)) last++;
+  }
   g.bufsz = 1;
   for (int d = 0; d < P.dim; d++) g.bufsz *= S[d];
   for (int d = 0; d < 3; d++) g.S[d] = S[d];
   g.str[P.dim - 1] = 1;
   for (int d = P.dim - 2; d >= 0; d--) g.str[d] = g.str[d + 1] * S[d + 1];
-  a.scale = (T)(P.hpw / P.sqd0);
-  a.inv_dx = (T)(1.0 / P.dx);
+  a.scale_d = P.hpw / P.sqd0;
+  a.inv_dx_d = 1.0 / P.dx;
+  a.hwdx_d = P.halfw / P.dx;
   a.halfw_over_dx = (T)(P.halfw / P.dx);
   a.beta = (T)P.beta;
-  a.inv_halfw = (T)(1.0 / P.halfw);
-  a.dx = (T)P.dx;
-  a.l0dx = (T)(P.l0 * P.dx);
+  a.dscale = (T)(a.inv_dx_d * a.scale_d / a.hwdx_d);
   a.inv_sqd0 = (T)(1.0 / P.sqd0);
   std::vector<T> twf(2 * G * NF), twh(2 * G * NH), tif(2 * NF * G), tih(2 * NH * G);
   for (int l = 0; l < G; l++) {
@@ -706,8 +786,6 @@ void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s
   up(tb.facf, facf);
   up(tb.faci, faci);
   up(tb.ts, ts);
-  tb.ts64.alloc(NF, s);
-  FGT_CUDA(cudaMemcpyAsync(tb.ts64.get(), P.ts.data(), sizeof(double) * NF, cudaMemcpyHostToDevice, s));
   FGT_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
   a.twf = tb.twf;
   a.twh = tb.twh;
@@ -720,9 +798,8 @@ void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s
 }
 
 template <typename T>
-size_t tw_bytes(const PWArgs<T>& a) {
-  const int K = a.g.K, G = a.g.G;
-  return sizeof(T) * 2 * (size_t)G * ((2 * K + 1) + (K + 1));
+size_t fixed_smem(const PWArgs<T>& a, int, int) {
+  return order_offset<T>(a.g.G, a.g.K);
 }
 
 template <typename KernelT>
@@ -732,9 +809,9 @@ void set_smem(KernelT k, size_t bytes) {
 
 template <typename T, int DIM, int W>
 int launch_form(PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>& gs, cudaStream_t s) {
-  size_t tw = tw_bytes(a);
-  size_t need = tw + sizeof(T) * (size_t)a.g.bufsz;
-  int grid = std::max(1, std::min(io.n_form, kSMs * 2));
+  size_t fix = fixed_smem(a, W, 1);
+  size_t need = fix + sizeof(T) * (size_t)a.g.bufsz;
+  int grid = std::max(1, std::min(io.n_form, kSMs));
   if (need <= (size_t)MAXSMEM) {
     auto k = k_form<T, DIM, W, false>;
     set_smem(k, need);
@@ -743,8 +820,8 @@ int launch_form(PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>& 
     gs.alloc((size_t)grid * a.g.bufsz, s);
     a.gscratch = gs;
     auto k = k_form<T, DIM, W, true>;
-    set_smem(k, tw);
-    k<<<grid, PW_THREADS, tw, s>>>(a, io, fp);
+    set_smem(k, fix);
+    k<<<grid, PW_THREADS, fix, s>>>(a, io, fp);
   }
   FGT_LAUNCH_CHECK();
   return 1;
@@ -752,19 +829,23 @@ int launch_form(PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>& 
 
 template <typename T, int DIM, int W>
 int launch_eval(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t s) {
-  size_t tw = tw_bytes(a);
-  size_t need = tw + sizeof(T) * (size_t)a.g.bufsz;
-  int grid = std::max(1, std::min(ep.nbox, kSMs * 2));
-  if (need <= (size_t)MAXSMEM) {
-    auto k = k_eval_nufft<T, DIM, W, false>;
-    set_smem(k, need);
-    k<<<grid, PW_THREADS, need, s>>>(a, ep);
-  } else {
+  size_t fix = fixed_smem(a, W, 2);
+  size_t need = fix + sizeof(T) * (size_t)a.g.bufsz;
+  int grid = std::max(1, std::min(ep.nbox, kSMs));
+  bool gb = need > (size_t)MAXSMEM;
+  if (gb) {
     gs.alloc((size_t)grid * a.g.bufsz, s);
     a.gscratch = gs;
-    auto k = k_eval_nufft<T, DIM, W, true>;
-    set_smem(k, tw);
-    k<<<grid, PW_THREADS, tw, s>>>(a, ep);
+  }
+  size_t sm = gb ? fix : need;
+  if (gb) {
+    auto k = k_eval_comp<T, DIM, W, true>;
+    set_smem(k, sm);
+    k<<<grid, PW_THREADS, sm, s>>>(a, ep);
+  } else {
+    auto k = k_eval_comp<T, DIM, W, false>;
+    set_smem(k, sm);
+    k<<<grid, PW_THREADS, sm, s>>>(a, ep);
   }
   FGT_LAUNCH_CHECK();
   return 1;
@@ -792,10 +873,82 @@ int eval_w(int w, PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t
     default: return launch_eval<T, DIM, 16>(a, ep, gs, s);
   }
 }
+template <typename T>
+int eval_dim(int dim, int w, PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t s) {
+  if (dim == 1) return eval_w<T, 1>(w, a, ep, gs, s);
+  if (dim == 2) return eval_w<T, 2>(w, a, ep, gs, s);
+  return eval_w<T, 3>(w, a, ep, gs, s);
+}
+
+void legendre(int nq, std::vector<double>& xq, std::vector<double>& wq) {
+  const double pi = 4.0 * atan(1.0);
+  xq.resize(nq);
+  wq.resize(nq);
+  for (int i = 0; i < nq; i++) {  // Newton on the Legendre polynomial
+    double x = cos(pi * (i + 0.75) / (nq + 0.5)), dp = 1;
+    for (int it = 0; it < 100; it++) {
+      double p0 = 1, p1 = x;
+      for (int j = 2; j <= nq; j++) {
+        double p2 = ((2 * j - 1) * x * p1 - (j - 1) * p0) / j;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = nq * (x * p1 - p0) / (x * x - 1);
+      double dxn = p1 / dp;
+      x -= dxn;
+      if (fabs(dxn) < 1e-16) break;
+    }
+    double p0 = 1, p1 = x;
+    for (int j = 2; j <= nq; j++) {
+      double p2 = ((2 * j - 1) * x * p1 - (j - 1) * p0) / j;
+      p0 = p1;
+      p1 = p2;
+    }
+    dp = nq * (x * p1 - p0) / (x * x - 1);
+    xq[i] = x;
+    wq[i] = 2 / ((1 - x * x) * dp * dp);
+  }
+}
 
 }  // namespace
 
 // ------------------------------------------------------------------ host set-up
+void pw_grid(PWParams& P, int w) {
+  const double pi = 4.0 * atan(1.0);
+  const int K = P.K, NF = 2 * K + 1;
+  w = supported_w(std::max(4, std::min(16, w)));
+  P.w = w;
+  P.beta = 0.97 * pi * (1 - 1.0 / (2 * 2.0)) * w;
+  P.halfw = w * P.dx / 2;
+  double xmax = (P.boxsize_cut / 2) * (P.hpw / P.sqd0) * (1 + 1e-6) + 1e-12;
+  int lmin = (int)ceil((-xmax - P.halfw) / P.dx);
+  int lmax = (int)ceil((xmax - P.halfw) / P.dx) + w - 1;
+  P.l0 = lmin;
+  P.G = lmax - lmin + 1;
+  P.wrap = false;
+  if (P.G >= P.nf) {
+    P.wrap = true;
+    P.G = P.nf;
+    P.l0 = 0;
+  }
+  // every in-place pass round needs one whole line per thread group
+  FGT_REQUIRE(std::max(P.G, NF) <= PW_THREADS, FGT_ERR_UNSUPPORTED,
+              "plane-wave expansion too long for the spreading kernels");
+  // Fourier transform of the kernel, Gauss-Legendre on [-halfw, halfw]
+  P.phihat.assign(NF, 0);
+  std::vector<double> xq, wq;
+  legendre(200, xq, wq);
+  for (int k = -K; k <= K; k++) {
+    double acc = 0;
+    for (size_t i = 0; i < xq.size(); i++) {
+      double z = xq[i];
+      double ph = exp(P.beta * (sqrt(std::max(0.0, 1 - z * z)) - 1));
+      acc += wq[i] * P.halfw * ph * cos(k * z * P.halfw);
+    }
+    P.phihat[k + K] = acc;
+  }
+}
+
 void pw_setup(PWParams& P, int dim, int nd, int npw, double pmax, int periodic_nodes, double bs0,
               double delta, double eps, double boxsize_cut, int spread_width) {
   const double pi = 4.0 * atan(1.0);
@@ -829,81 +982,35 @@ void pw_setup(PWParams& P, int dim, int nd, int npw, double pmax, int periodic_n
   P.wsym[0] = P.wsym[2 * K] = ws[0] / 2;  // split the k=-K term over +-K
   P.hpw = h;
   P.sqd0 = sqrt(P.delta0);
+  P.boxsize_cut = boxsize_cut;
   P.xmin = boxsize_cut / P.sqd0;
   // spreading grid (upsampling 2 over the 2K+1 modes), ES kernel
-  P.nf = 2 * NF + (2 * NF) % 2;
+  P.nf = 2 * NF;
   P.dx = 2 * pi / P.nf;
   int w = spread_width > 0 ? spread_width : (int)ceil(log10(1.0 / eps)) + 2;
-  w = std::max(4, std::min(16, w));
-  w = supported_w(w);
-  P.w = w;
-  P.beta = 0.97 * pi * (1 - 1.0 / (2 * 2.0)) * w;
-  P.halfw = w * P.dx / 2;
-  double xmax = (boxsize_cut / 2) * (P.hpw / P.sqd0) * (1 + 1e-6) + 1e-12;
-  int lmin = (int)ceil((-xmax - P.halfw) / P.dx);
-  int lmax = (int)ceil((xmax - P.halfw) / P.dx) + w - 1;
-  P.l0 = lmin;
-  P.G = lmax - lmin + 1;
-  P.wrap = false;
-  if (P.G >= P.nf) {
-    P.wrap = true;
-    P.G = P.nf;
-    P.l0 = 0;
-  }
-  // every in-place pass round needs one whole line per thread group
-  FGT_REQUIRE(std::max(P.G, NF) <= PW_THREADS, FGT_ERR_UNSUPPORTED,
-              "plane-wave expansion too long for the spreading kernels");
-  // Fourier transform of the kernel, Gauss-Legendre on [0, halfw]
-  P.phihat.assign(NF, 0);
-  const int nq = 200;
-  std::vector<double> xq(nq), wq(nq);
-  for (int i = 0; i < nq; i++) {  // Newton on Legendre polynomials
-    double x = cos(pi * (i + 0.75) / (nq + 0.5));
-    for (int it = 0; it < 100; it++) {
-      double p0 = 1, p1 = x;
-      for (int j = 2; j <= nq; j++) {
-        double p2 = ((2 * j - 1) * x * p1 - (j - 1) * p0) / j;
-        p0 = p1;
-        p1 = p2;
-      }
-      double dp = nq * (x * p1 - p0) / (x * x - 1);
-      double dxn = p1 / dp;
-      x -= dxn;
-      if (fabs(dxn) < 1e-16) break;
-    }
-    double p0 = 1, p1 = x;
-    for (int j = 2; j <= nq; j++) {
-      double p2 = ((2 * j - 1) * x * p1 - (j - 1) * p0) / j;
-      p0 = p1;
-      p1 = p2;
-    }
-    double dp = nq * (x * p1 - p0) / (x * x - 1);
-    xq[i] = x;
-    wq[i] = 2 / ((1 - x * x) * dp * dp);
-  }
-  for (int k = -K; k <= K; k++) {
-    double acc = 0;
-    for (int i = 0; i < nq; i++) {
-      double t = xq[i] * P.halfw;  // over [-halfw, halfw]
-      double z = xq[i];
-      double ph = exp(P.beta * (sqrt(std::max(0.0, 1 - z * z)) - 1));
-      acc += wq[i] * P.halfw * ph * cos(k * t);
-    }
-    P.phihat[k + K] = acc;
-  }
+  pw_grid(P, w);
 }
 
 // ------------------------------------------------------------------ drivers
+double pw_pass_flops(const PWParams& P) {
+  const double G = P.G, NF = 2 * P.K + 1, NH = P.K + 1;
+  double fma;
+  if (P.dim == 3) fma = G * G * NH * G * 2 + G * NH * NF * G * 4 + NF * NH * NF * G * 4;
+  else if (P.dim == 2) fma = G * NH * G * 2 + NH * NF * G * 4;
+  else fma = NH * G * 2;
+  return 2 * fma;
+}
+
 template <typename T>
 int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>& src,
-            PWData<T>& D, cudaStream_t s) {
+            PWData<T>& D, PWWork* work, cudaStream_t s) {
   if (L.n_form <= 0) {
     D.mp.alloc(2, s);
     return 0;
   }
   PWArgs<T> a;
   DevTables<T> tb;
-  make_args<T>(P, a, tb, s);
+  make_args<T>(P, a, tb, s, false);
   D.mp.alloc((size_t)L.n_form * P.nd * 2 * P.nexp, s);
   FormIO io;
   io.n_form = L.n_form;
@@ -926,11 +1033,24 @@ int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>
   if (P.dim == 1) n = form_w<T, 1>(P.w, a, io, fp, gs, s);
   else if (P.dim == 2) n = form_w<T, 2>(P.w, a, io, fp, gs, s);
   else n = form_w<T, 3>(P.w, a, io, fp, gs, s);
+  if (work) {
+    DBuf<unsigned long long> c(1, s);
+    c.zero();
+    k_count_points<<<grid_for(L.n_form, 256), 256, 0, s>>>(L.n_form, L.form_box, src.lo, src.hi, c);
+    FGT_LAUNCH_CHECK();
+    unsigned long long h = 0;
+    FGT_CUDA(cudaMemcpyAsync(&h, c.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FGT_CUDA(cudaStreamSynchronize(s));
+    const double wd = pow((double)P.w, P.dim), tr = (double)io.ncomp * P.nd;
+    work->pts_form = (double)h;
+    work->flops_form = tr * (L.n_form * pw_pass_flops(P) + (double)h * 2 * wd);
+    n++;
+  }
   return n;
 }
 
 template <typename T>
-int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, cudaStream_t s) {
+int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, PWWork* work, cudaStream_t s) {
   int nsh = P.dim == 1 ? 3 : (P.dim == 2 ? 9 : 27);
   D.wtab.alloc((size_t)nsh * 2 * P.nexp, s);
   DBuf<double> ts64(P.ts.size(), s);
@@ -940,10 +1060,11 @@ int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, cudaStream_t s
                                                                    P.xmin, D.wtab);
   FGT_LAUNCH_CHECK();
   D.loc.alloc((size_t)std::max(L.n_eval, 1) * P.nd * 2 * P.nexp, s);
+  if (work)
+    work->bytes_translate = (double)sizeof(T) * 2 * P.nexp * P.nd *
+                            ((double)L.n_trans + 2.0 * L.n_eval);
   if (L.n_eval == 0) return 1;
-  FGT_REQUIRE(L.n_eval < 65536 * 32, FGT_ERR_UNSUPPORTED, "too many expansion boxes");
   int gx = std::max(1, std::min(ceil_div(P.nexp, 256), 64));
-  // grid.y limited to 65535: process in slabs
   for (int e0 = 0; e0 < L.n_eval; e0 += 65535) {
     int ne = std::min(65535, L.n_eval - e0);
     dim3 grid(gx, ne);
@@ -958,20 +1079,30 @@ int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, cudaStream_t s
 
 template <typename T>
 int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D,
-            const EvalSet<T>& e0, const EvalSet<T>& e1, int small_eval, int* n_nufft,
+            const EvalSet<T>& e0, const EvalSet<T>& e1, int small_eval, PWWork* work,
             cudaStream_t s) {
   // both evaluation sets (sources, targets) share the grid of every box
   const bool u0 = e0.pgh > 0 && e0.n > 0, u1 = e1.pgh > 0 && e1.n > 0;
   if (!(u0 || u1) || L.n_eval <= 0) return 0;
+  const int pgh_max = std::max(u0 ? e0.pgh : 0, u1 ? e1.pgh : 0);
+  // grid of the evaluation: pot (w), pot+grad through the kernel derivative
+  // (w+2), or one grid per component when hessians are requested (w)
+  // one grid per output component (pot, grad_k, hess_kl), thread-per-point
+  // interpolation in bank-balanced order
+  (void)pgh_max;
+  const int mode = 2;
+  PWParams Pe = P;
   PWArgs<T> a;
   DevTables<T> tb;
-  make_args<T>(P, a, tb, s);
+  make_args<T>(Pe, a, tb, s, false);
   int launches = 0;
   const int thr = small_eval >= 0 ? small_eval : (P.dim == 3 ? 48 : (P.dim == 2 ? 8 : 4));
   DBuf<int> big(L.n_eval, s), pos(L.n_eval, s), tot(1, s);
+  DBuf<unsigned long long> cnt(2, s);
+  cnt.zero();
   k_eval_split<<<grid_for(L.n_eval, 256), 256, 0, s>>>(
       L.n_eval, L.eval_box, u0 ? e0.lo : nullptr, u0 ? e0.hi : nullptr, u1 ? e1.lo : nullptr,
-      u1 ? e1.hi : nullptr, thr, big);
+      u1 ? e1.hi : nullptr, thr, big, cnt);
   FGT_LAUNCH_CHECK();
   exclusive_scan_i32(big, pos, L.n_eval, tot, s);
   int nbig = fetch_int(tot, s);
@@ -1000,10 +1131,8 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   if (nbig > 0) {
     ep.boxes = lbig;
     ep.nbox = nbig;
-    if (P.dim == 1) launches += eval_w<T, 1>(P.w, a, ep, gs, s);
-    else if (P.dim == 2) launches += eval_w<T, 2>(P.w, a, ep, gs, s);
-    else launches += eval_w<T, 3>(P.w, a, ep, gs, s);
-    if (n_nufft) *n_nufft += nbig;
+    launches += eval_dim<T>(P.dim, Pe.w, a, ep, gs, s);
+    if (work) work->n_nufft += nbig;
   }
   int nsmall = L.n_eval - nbig;
   if (nsmall > 0) {
@@ -1011,26 +1140,43 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
     ep.nbox = nsmall;
     int grid = std::max(1, std::min(nsmall, kSMs * 8));
     size_t sm = sizeof(T) * 2 * P.dim * (2 * P.K + 1);
-    if (P.dim == 1) k_eval_modal<T, 1><<<grid, PW_THREADS, sm, s>>>(a, ep);
-    else if (P.dim == 2) k_eval_modal<T, 2><<<grid, PW_THREADS, sm, s>>>(a, ep);
-    else k_eval_modal<T, 3><<<grid, PW_THREADS, sm, s>>>(a, ep);
+    if (P.dim == 1) k_eval_modal<T, 1><<<grid, MODAL_THREADS, sm, s>>>(a, ep);
+    else if (P.dim == 2) k_eval_modal<T, 2><<<grid, MODAL_THREADS, sm, s>>>(a, ep);
+    else k_eval_modal<T, 3><<<grid, MODAL_THREADS, sm, s>>>(a, ep);
     FGT_LAUNCH_CHECK();
     launches++;
+  }
+  if (work) {
+    unsigned long long h[2] = {0, 0};
+    FGT_CUDA(cudaMemcpyAsync(h, cnt.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FGT_CUDA(cudaStreamSynchronize(s));
+    const double wd = pow((double)Pe.w, P.dim);
+    const double grids = mode == 2 ? ep.ncomp_max : 1;
+    const double fl_pt = mode == 1 ? 4.0 * wd : 2.0 * wd * grids;
+    work->pts_nufft = (double)h[0];
+    work->pts_modal = (double)h[1];
+    work->flops_eval = (double)P.nd * (nbig * grids * pw_pass_flops(Pe) + (double)h[0] * fl_pt) +
+                       (double)P.nd * ep.ncomp_max * (double)h[1] * P.nexp * 8.0;
+    work->w_eval = Pe.w;
+    work->G_eval = Pe.G;
   }
   FGT_CUDA(cudaStreamSynchronize(s));  // tables lifetime
   return launches;
 }
 
 template int pw_form<float>(const PWParams&, const Tree&, const Lists&, const SourceSet<float>&,
-                            PWData<float>&, cudaStream_t);
+                            PWData<float>&, PWWork*, cudaStream_t);
 template int pw_form<double>(const PWParams&, const Tree&, const Lists&, const SourceSet<double>&,
-                             PWData<double>&, cudaStream_t);
-template int pw_translate<float>(const PWParams&, const Lists&, PWData<float>&, cudaStream_t);
-template int pw_translate<double>(const PWParams&, const Lists&, PWData<double>&, cudaStream_t);
+                             PWData<double>&, PWWork*, cudaStream_t);
+template int pw_translate<float>(const PWParams&, const Lists&, PWData<float>&, PWWork*,
+                                 cudaStream_t);
+template int pw_translate<double>(const PWParams&, const Lists&, PWData<double>&, PWWork*,
+                                  cudaStream_t);
 template int pw_eval<float>(const PWParams&, const Tree&, const Lists&, const PWData<float>&,
-                            const EvalSet<float>&, const EvalSet<float>&, int, int*, cudaStream_t);
+                            const EvalSet<float>&, const EvalSet<float>&, int, PWWork*,
+                            cudaStream_t);
 template int pw_eval<double>(const PWParams&, const Tree&, const Lists&, const PWData<double>&,
-                             const EvalSet<double>&, const EvalSet<double>&, int, int*,
+                             const EvalSet<double>&, const EvalSet<double>&, int, PWWork*,
                              cudaStream_t);
 
 }  // namespace fgt

@@ -29,6 +29,7 @@ struct PWParams {
   std::vector<double> wsym; // symmetrised weights, index k+K
   std::vector<double> phihat;  // FT of the spreading kernel at k = -K..K
   double xmin = 0;          // box size at the cutoff level / sqrt(delta0)
+  double boxsize_cut = 0;   // box size at the cutoff level
 };
 
 // Host set-up of the plane-wave parameters (FP64): nodes and weights of
@@ -36,6 +37,8 @@ struct PWParams {
 // and kernel of the spreader, kernel Fourier transform by quadrature.
 void pw_setup(PWParams& P, int dim, int nd, int npw, double pmax, int periodic_nodes,
               double bs0, double delta, double eps, double boxsize_cut, int spread_width);
+// (Re)computes the width-dependent grid of P (kernel width w cells).
+void pw_grid(PWParams& P, int w);
 
 template <typename T>
 struct PWData {
@@ -44,15 +47,22 @@ struct PWData {
   DBuf<T> wtab;  // [3^dim][nexp] complex shift tables
 };
 
+// Algorithmic work counters of one call (optional).
+struct PWWork {
+  double pts_form = 0, pts_nufft = 0, pts_modal = 0;
+  double flops_form = 0, flops_eval = 0, bytes_translate = 0;
+  int n_nufft = 0, w_eval = 0, G_eval = 0;
+};
+
 // Forms the expansions of all form boxes.  Returns launches.
 template <typename T>
 int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>& src,
-            PWData<T>& D, cudaStream_t s);
+            PWData<T>& D, PWWork* work, cudaStream_t s);
 template <typename T>
-int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, cudaStream_t s);
+int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, PWWork* work, cudaStream_t s);
 template <typename T>
 int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D,
-            const EvalSet<T>& e0, const EvalSet<T>& e1, int small_eval, int* n_nufft,
+            const EvalSet<T>& e0, const EvalSet<T>& e1, int small_eval, PWWork* work,
             cudaStream_t s);
 
 }  // namespace fgt

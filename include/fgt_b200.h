@@ -52,6 +52,12 @@ typedef struct fgt_stats {
   int grid_cells;        /* spreading sub-grid cells per dimension */
   int n_kernel_launches; /* kernels launched by this call */
   double near_pairs;     /* source/target pairs of the direct near field */
+  /* algorithmic work of the call (FP32 or FP64 flops, HBM bytes) */
+  double flops_form;     /* spreading stencils + DFT passes of the form kernel */
+  double flops_eval;     /* DFT passes + interpolation stencils + modal sums */
+  double flops_direct;   /* near-field pair arithmetic */
+  double bytes_translate;/* expansion traffic of the translation kernel */
+  double pts_form, pts_eval_nufft, pts_eval_modal;
   double bs0, cen0[3];
   /* milliseconds on the device stream: 0 h2d, 1 tree, 2 sort+gather,
    * 3 lists, 4 form, 5 translate, 6 eval, 7 direct, 8 scatter, 9 d2h,

@@ -108,8 +108,14 @@ def tree(dim, delta, eps, iperiod, sources, targets, bs0=1.0, cen0=None, ndiv=0)
 
 def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None,
          rnormal=None, ifpgh=1, targets=None, ifpghtarg=0, bs0=1.0, cen0=None,
-         quirks=0):
-    """Restated reference pfgt; returns dict(pot, grad, hess, pottarg, ...)."""
+         quirks=0, nufft="exact"):
+    """Restated reference pfgt; returns dict(pot, grad, hess, pottarg, ...).
+
+    nufft="exact": plane-wave sums by exact non-uniform DFTs (the checker);
+    nufft="spread": the restatement's own ES-kernel NUFFT, OpenMP over boxes
+    (the timed CPU baseline).  quirks: bit 0/1/2 reproduce the reference's
+    ifpgh==ifpghtarg skip, nd>1 scramble and empty small-root result.
+    """
     L = lib()
     src = _f64(sources).reshape(-1, dim)
     ns = src.shape[0]
@@ -134,7 +140,7 @@ def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None,
                   C.c_int(ifcharge), _p(q), C.c_int(ifdipole), _p(rn), _p(ds),
                   C.c_int(ifpgh), _p(pot), _p(grad), _p(hess), C.c_int(nt),
                   _p(trg if nt else np.zeros(1)), C.c_int(ifpghtarg), _p(pt), _p(gt),
-                  _p(ht), C.c_int(quirks))
+                  _p(ht), C.c_int(quirks), C.c_int(1 if nufft == "spread" else 0))
     out = dict(bs0=b0.value, cen0=c0[:dim].copy())
     if ifpgh >= 1:
         out["pot"] = pot[:ns]
@@ -149,6 +155,11 @@ def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None,
     if ifpghtarg >= 3:
         out["hesstarg"] = ht[:nt]
     return out
+
+
+def threads():
+    """OpenMP threads the restatement uses."""
+    return int(lib().oracle_threads())
 
 
 def direct_exact(nd, dim, delta, sources, evalpts, charge=None, dipstr=None,

@@ -777,6 +777,253 @@ static void eval_pw(int nd, int dim, double delta0, const double *cen, double hp
   free(fk);
 }
 
+/* ------------------------------------------------------------------------ */
+/* fast NUFFT (timed CPU baseline): exponential-of-semicircle spreading on  */
+/* the sub-grid the box's points reach, separable DFT passes, FP64.         */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int npw, nf, w, G, l0, wrap;
+  double dx, halfw, beta;
+  double *phihat; /* modes j = -npw/2 .. npw/2-1 */
+  zcplx *tw;      /* tw[l*npw + m] = exp(-i (m-npw/2) x_l), x_l = (l0+l) dx */
+} fastnufft;
+
+static void fast_setup(fastnufft *F, int npw, double eps, double xmax) {
+  const double pi = 4.0 * atan(1.0);
+  int w = (int)ceil(log10(1.0 / eps)) + 2, i, m, l;
+  if (w < 4) w = 4;
+  if (w > 16) w = 16;
+  F->npw = npw;
+  F->nf = 2 * (npw + 1);
+  F->w = w;
+  F->dx = 2 * pi / F->nf;
+  F->halfw = w * F->dx / 2;
+  F->beta = 0.97 * pi * 0.75 * w;
+  xmax = xmax * (1 + 1e-6) + 1e-12;
+  int lmin = (int)ceil((-xmax - F->halfw) / F->dx);
+  int lmax = (int)ceil((xmax - F->halfw) / F->dx) + w - 1;
+  F->l0 = lmin;
+  F->G = lmax - lmin + 1;
+  F->wrap = 0;
+  if (F->G >= F->nf) { F->wrap = 1; F->G = F->nf; F->l0 = 0; }
+  F->phihat = xmalloc(sizeof(double) * npw);
+  /* midpoint quadrature of the kernel transform (smooth, compact) */
+  const int nq = 400;
+  for (m = 0; m < npw; m++) {
+    double k = m - npw / 2, acc = 0;
+    for (i = 0; i < nq; i++) {
+      double z = -1 + (i + 0.5) * 2.0 / nq;
+      acc += exp(F->beta * (sqrt(1 - z * z) - 1)) * cos(k * z * F->halfw);
+    }
+    F->phihat[m] = acc * F->halfw * 2.0 / nq;
+  }
+  F->tw = xmalloc(sizeof(zcplx) * F->G * npw);
+  for (l = 0; l < F->G; l++)
+    for (m = 0; m < npw; m++)
+      F->tw[l * npw + m] = cexp(-I * (double)(m - npw / 2) * (F->l0 + l) * F->dx);
+}
+static void fast_free(fastnufft *F) { free(F->phihat); free(F->tw); }
+
+/* cells and kernel values of one coordinate */
+static void fast_row(const fastnufft *F, double x, int *idx, double *phi) {
+  double u = x / F->dx;
+  int i0 = (int)ceil(u - F->halfw / F->dx), j;
+  for (j = 0; j < F->w; j++) {
+    double z = ((i0 + j) - u) * F->dx / F->halfw, v = 1 - z * z;
+    phi[j] = exp(F->beta * (sqrt(v > 0 ? v : 0) - 1));
+    int c = i0 + j;
+    if (F->wrap) { c %= F->nf; if (c < 0) c += F->nf; }
+    else {
+      c -= F->l0;
+      if (c < 0) c = 0;
+      if (c >= F->G) c = F->G - 1;
+    }
+    idx[j] = c;
+  }
+}
+
+/* separable transform of a dim-D array along every axis: in[G..] -> out[npw..]
+ * (forward, sign -) or out[G..] from in[npw..] (inverse, sign +). */
+static void fast_dft(const fastnufft *F, int dim, const zcplx *in, zcplx *out, int inverse) {
+  int G = F->G, P = F->npw, d, nin = inverse ? P : G, nout = inverse ? G : P;
+  size_t tot = 1;
+  for (d = 0; d < dim; d++) tot *= (size_t)(nin > nout ? nin : nout);
+  zcplx *a = xcalloc(tot, sizeof(zcplx)), *b = xcalloc(tot, sizeof(zcplx));
+  int ext[MAXDIM];
+  for (d = 0; d < dim; d++) ext[d] = nin;
+  size_t n0 = 1;
+  for (d = 0; d < dim; d++) n0 *= nin;
+  memcpy(a, in, sizeof(zcplx) * n0);
+  for (d = 0; d < dim; d++) { /* transform axis d (axis 0 fastest) */
+    size_t inner = 1, outer = 1, i, o, j;
+    int k;
+    for (k = 0; k < d; k++) inner *= ext[k];
+    for (k = d + 1; k < dim; k++) outer *= ext[k];
+    for (o = 0; o < outer; o++)
+      for (i = 0; i < inner; i++)
+        for (j = 0; j < (size_t)nout; j++) {
+          zcplx acc = 0;
+          int l;
+          for (l = 0; l < nin; l++) {
+            zcplx t = inverse ? conj(F->tw[(size_t)j * P + l]) : F->tw[(size_t)l * P + j];
+            acc += a[(o * nin + l) * inner + i] * t;
+          }
+          b[(o * nout + j) * inner + i] = acc;
+        }
+    ext[d] = nout;
+    zcplx *t = a; a = b; b = t;
+  }
+  size_t nres = 1;
+  for (d = 0; d < dim; d++) nres *= nout;
+  memcpy(out, a, sizeof(zcplx) * nres);
+  free(a);
+  free(b);
+}
+
+/* type-1 sums fk(k) = sum_j c_j exp(-i k.x_j), modes -npw/2..npw/2-1 (x fastest) */
+static void fast_type1(const fastnufft *F, int dim, int n, const double *x /* scaled, n*dim */,
+                       const double *c, zcplx *fk) {
+  int G = F->G, P = F->npw, w = F->w, j, a, b2, e;
+  size_t ng = 1, m, nexp = 1;
+  int d;
+  for (d = 0; d < dim; d++) { ng *= G; nexp *= P; }
+  zcplx *g = xcalloc(ng, sizeof(zcplx));
+  int idx[MAXDIM][16];
+  double ph[MAXDIM][16];
+  for (j = 0; j < n; j++) {
+    for (d = 0; d < dim; d++) fast_row(F, x[(size_t)j * dim + d], idx[d], ph[d]);
+    if (dim == 1) {
+      for (a = 0; a < w; a++) g[idx[0][a]] += c[j] * ph[0][a];
+    } else if (dim == 2) {
+      for (b2 = 0; b2 < w; b2++)
+        for (a = 0; a < w; a++) g[(size_t)idx[1][b2] * G + idx[0][a]] += c[j] * ph[0][a] * ph[1][b2];
+    } else {
+      for (e = 0; e < w; e++)
+        for (b2 = 0; b2 < w; b2++)
+          for (a = 0; a < w; a++)
+            g[((size_t)idx[2][e] * G + idx[1][b2]) * G + idx[0][a]] +=
+                c[j] * ph[0][a] * ph[1][b2] * ph[2][e];
+    }
+  }
+  fast_dft(F, dim, g, fk, 0);
+  for (m = 0; m < nexp; m++) {
+    size_t r = m;
+    double f = 1;
+    for (d = 0; d < dim; d++) { f *= F->dx / F->phihat[r % P]; r /= P; }
+    fk[m] *= f;
+  }
+  free(g);
+}
+
+/* type-2 values Re sum_k fk(k) exp(+i k.x_j) at n scaled points */
+static void fast_type2(const fastnufft *F, int dim, const zcplx *fk, int n, const double *x,
+                       double *out) {
+  int G = F->G, P = F->npw, w = F->w, j, a, b2, e, d;
+  size_t ng = 1, m, nexp = 1;
+  for (d = 0; d < dim; d++) { ng *= G; nexp *= P; }
+  zcplx *h = xmalloc(sizeof(zcplx) * nexp), *g = xmalloc(sizeof(zcplx) * ng);
+  for (m = 0; m < nexp; m++) {
+    size_t r = m;
+    double f = 1;
+    for (d = 0; d < dim; d++) { f *= F->dx / F->phihat[r % P]; r /= P; }
+    h[m] = fk[m] * f;
+  }
+  fast_dft(F, dim, h, g, 1);
+  int idx[MAXDIM][16];
+  double ph[MAXDIM][16];
+  for (j = 0; j < n; j++) {
+    double acc = 0;
+    for (d = 0; d < dim; d++) fast_row(F, x[(size_t)j * dim + d], idx[d], ph[d]);
+    if (dim == 1) {
+      for (a = 0; a < w; a++) acc += creal(g[idx[0][a]]) * ph[0][a];
+    } else if (dim == 2) {
+      for (b2 = 0; b2 < w; b2++)
+        for (a = 0; a < w; a++) acc += creal(g[(size_t)idx[1][b2] * G + idx[0][a]]) * ph[0][a] * ph[1][b2];
+    } else {
+      for (e = 0; e < w; e++)
+        for (b2 = 0; b2 < w; b2++)
+          for (a = 0; a < w; a++)
+            acc += creal(g[((size_t)idx[2][e] * G + idx[1][b2]) * G + idx[0][a]]) * ph[0][a] *
+                   ph[1][b2] * ph[2][e];
+    }
+    out[j] = acc;
+  }
+  free(h);
+  free(g);
+}
+
+/* gnd_formpw with the fast type-1 transform */
+static void form_pw_fast(const fastnufft *F, int nd, int dim, double delta0, const double *src,
+                         int n, int ifcharge, const double *q, int ifdipole, const double *rn,
+                         const double *ds, const double *cen, double hpw, int npw,
+                         const double *ws, const double *ts, zcplx *ffexp) {
+  int nexp = ipow(npw, dim), j, k, id, m;
+  double dsq = hpw / sqrt(delta0), dsq0 = 1 / sqrt(delta0);
+  double *x = xmalloc(sizeof(double) * (size_t)n * dim + 8), *c = xmalloc(sizeof(double) * (n + 1));
+  zcplx *fk = xmalloc(sizeof(zcplx) * nexp);
+  for (j = 0; j < n; j++)
+    for (k = 0; k < dim; k++) x[(size_t)j * dim + k] = (src[(size_t)j * dim + k] - cen[k]) * dsq;
+  for (m = 0; m < nexp * nd; m++) ffexp[m] = 0;
+  for (id = 0; id < nd; id++) {
+    int comp;
+    for (comp = 0; comp <= dim; comp++) {
+      if (comp == 0 && !ifcharge) continue;
+      if (comp > 0 && !ifdipole) break;
+      for (j = 0; j < n; j++)
+        c[j] = comp == 0 ? q[(size_t)j * nd + id]
+                         : ds[(size_t)j * nd + id] * rn[(size_t)j * dim + comp - 1];
+      fast_type1(F, dim, n, x, c, fk);
+      for (m = 0; m < nexp; m++) {
+        int r = m, mi[MAXDIM];
+        double wsum = 1;
+        for (k = 0; k < dim; k++) { mi[k] = r % npw; r /= npw; wsum *= ws[mi[k]]; }
+        zcplx f = comp == 0 ? wsum : wsum * ts[mi[comp - 1]] * (-I * dsq0);
+        ffexp[(size_t)id * nexp + m] += f * fk[m];
+      }
+    }
+  }
+  free(x); free(c); free(fk);
+}
+
+/* gnd_pweval with the fast type-2 transform (no quirks) */
+static void eval_pw_fast(const fastnufft *F, int nd, int dim, double delta0, const double *cen,
+                         double hpw, int npw, const double *ts, const zcplx *pwexp,
+                         const double *xin, int n, int ifpgh, double *pot, double *grad,
+                         double *hess) {
+  int nexp = ipow(npw, dim), j, k, id, m, l, nhess = dim * (dim + 1) / 2;
+  int kend = (ifpgh == 1) ? 0 : (ifpgh == 2 ? dim : dim + nhess);
+  double dsq = hpw / sqrt(delta0), z = 1 / sqrt(delta0);
+  double *x = xmalloc(sizeof(double) * (size_t)n * dim + 8), *v = xmalloc(sizeof(double) * (n + 1));
+  zcplx *fk = xmalloc(sizeof(zcplx) * nexp);
+  for (j = 0; j < n; j++)
+    for (k = 0; k < dim; k++) x[(size_t)j * dim + k] = (xin[(size_t)j * dim + k] - cen[k]) * dsq;
+  for (id = 0; id < nd; id++)
+    for (l = 0; l <= kend; l++) {
+      int pa = 0, pb = 0;
+      if (l > dim) {
+        int hm = l - 1 - dim;
+        if (dim == 2) { pa = hm == 2 ? 1 : 0; pb = hm == 0 ? 0 : 1; }
+        else if (dim == 3) { pa = hm < 3 ? hm : (hm < 5 ? 0 : 1); pb = hm < 3 ? hm : (hm == 3 ? 1 : 2); }
+      }
+      for (m = 0; m < nexp; m++) {
+        int r = m, mi[MAXDIM];
+        for (k = 0; k < dim; k++) { mi[k] = r % npw; r /= npw; }
+        zcplx p = pwexp[(size_t)id * nexp + m];
+        if (l == 0) fk[m] = p;
+        else if (l <= dim) fk[m] = p * ts[mi[l - 1]] * (I * z);
+        else fk[m] = -p * ts[mi[pa]] * ts[mi[pb]] * z * z;
+      }
+      fast_type2(F, dim, fk, n, x, v);
+      for (j = 0; j < n; j++) {
+        if (l == 0) pot[(size_t)j * nd + id] += v[j];
+        else if (l <= dim) grad[((size_t)j * dim + (l - 1)) * nd + id] += v[j];
+        else hess[((size_t)j * nhess + (l - 1 - dim)) * nd + id] += v[j];
+      }
+    }
+  free(x); free(v); free(fk);
+}
+
 /* gnd_mk_full_translation_matrices, pfgt_nufftrouts.f:336-424 (nmax = 1):
  * W[s][m] = prod_d exp(i ts(m_d) xmin s_d), shift index s = sum_d
  * (s_d+1) 3^d with dimension 0 fastest (gnd_find_pwshift_ind order). */
@@ -1022,7 +1269,7 @@ int oracle_pfgt(int nd, int dim, double delta, double eps, int iperiod,
                 const double *rnormal, const double *dipstr, int ifpgh,
                 double *pot, double *grad, double *hess, int nt,
                 const double *targ, int ifpghtarg, double *pottarg,
-                double *gradtarg, double *hesstarg, int quirks) {
+                double *gradtarg, double *hesstarg, int quirks, int nufft_mode) {
   int k, i, b, id, nhess = dim * (dim + 1) / 2;
   double cen0[MAXDIM] = {0, 0, 0};
   for (k = 0; k < dim; k++) cen0[k] = cen0_io[k];
@@ -1075,8 +1322,23 @@ int oracle_pfgt(int nd, int dim, double delta, double eps, int iperiod,
   double hpw = tsn[npw / 2 + 1];
   int nlevend = nlevels;
   if (npwlevel <= nlevels) nlevend = npwlevel;
+  int do_pw = npwlevel < nlevels;
+  /* A root smaller than half the cut-off with ns <= ndiv forms no expansion
+   * and the reference returns zeros (pfgt.f:649-650, 779); unless that quirk
+   * is requested, compute its direct self interaction. */
+  if (!(quirks & 4) && npwlevel < 0 && ns <= ndiv) {
+    do_pw = 0;
+    nlevend = 0;
+    r->nlist1[0] = 1;
+    r->list1[0] = 0;
+  }
+  fastnufft FN;
+  if (nufft_mode == 1 && do_pw) {
+    double xmax = (r->boxsize[ncutoff] / 2) * hpw / sqrt(delta0);
+    fast_setup(&FN, npw, eps, xmax);
+  }
 
-  if (npwlevel < nlevels) {
+  if (do_pw) {
     int nexp = ipow(npw, dim);
     int nshift = ipow(3, dim);
     zcplx *W = xmalloc(sizeof(zcplx) * (size_t)nexp * nshift);
@@ -1090,9 +1352,17 @@ int oracle_pfgt(int nd, int dim, double delta, double eps, int iperiod,
         loc[b] = xcalloc((size_t)nexp * nd, sizeof(zcplx));
       }
     /* step 1: form, pfgt.f:764-798 */
+#pragma omp parallel for schedule(dynamic)
     for (b = f; b <= l; b++) {
       int is = r->isrcse[2 * b], npts = r->isrcse[2 * b + 1] - is + 1;
-      if (npts > ndiv) {
+      if (npts > ndiv && nufft_mode == 1) {
+        form_pw_fast(&FN, nd, dim, delta0, &ss[(size_t)is * dim], npts, ifcharge,
+                     ifcharge ? &qs[(size_t)is * nd] : NULL, ifdipole,
+                     ifdipole ? &rns[(size_t)is * dim] : NULL,
+                     ifdipole ? &dss[(size_t)is * nd] : NULL, &r->centers[b * dim], hpw,
+                     npw, ws, tsn, mp[b]);
+        memcpy(loc[b], mp[b], sizeof(zcplx) * (size_t)nexp * nd);
+      } else if (npts > ndiv) {
         form_pw(nd, dim, delta0, &ss[(size_t)is * dim], npts, ifcharge,
                 ifcharge ? &qs[(size_t)is * nd] : NULL, ifdipole,
                 ifdipole ? &rns[(size_t)is * dim] : NULL,
@@ -1102,6 +1372,7 @@ int oracle_pfgt(int nd, int dim, double delta, double eps, int iperiod,
       }
     }
     /* step 2: mp -> loc, pfgt.f:818-835 */
+#pragma omp parallel for schedule(dynamic) private(i)
     for (b = f; b <= l; b++)
       for (i = 0; i < r->nlistpw[b]; i++) {
         int jb = r->listpw[(size_t)b * r->mlistpw + i];
@@ -1112,6 +1383,7 @@ int oracle_pfgt(int nd, int dim, double delta, double eps, int iperiod,
           loc[b][m] += mp[jb][m] * W[(size_t)ind * nexp + m % nexp];
       }
     /* step 3: eval, pfgt.f:880-1062 */
+#pragma omp parallel for schedule(dynamic)
     for (b = f; b <= l; b++) {
       if (!r->ifpwexp[b]) continue;
       int its = r->itrgse[2 * b], nts = r->itrgse[2 * b + 1] - its + 1;
@@ -1121,6 +1393,17 @@ int oracle_pfgt(int nd, int dim, double delta, double eps, int iperiod,
         /* multi-threaded branch of pfgt.f:938-958 */
         do_t = (nts > 0 && nss == 0);
         do_s = (nss > 0 && nts == 0);
+      }
+      if (nufft_mode == 1 && !(quirks & 2)) {
+        if (do_t && nts > 0 && ifpghtarg > 0)
+          eval_pw_fast(&FN, nd, dim, delta0, &r->centers[b * dim], hpw, npw, tsn, loc[b],
+                       &ts_[(size_t)its * dim], nts, ifpghtarg, &pt[(size_t)its * nd],
+                       &gt[(size_t)its * nd * dim], &ht[(size_t)its * nd * nhess]);
+        if (do_s && nss > 0 && ifpgh > 0)
+          eval_pw_fast(&FN, nd, dim, delta0, &r->centers[b * dim], hpw, npw, tsn, loc[b],
+                       &ss[(size_t)iss * dim], nss, ifpgh, &ps[(size_t)iss * nd],
+                       &gs[(size_t)iss * nd * dim], &hs[(size_t)iss * nd * nhess]);
+        continue;
       }
       if (do_t && nts > 0 && ifpghtarg > 0)
         eval_pw(nd, dim, delta0, &r->centers[b * dim], hpw, npw, tsn, loc[b],
@@ -1133,11 +1416,13 @@ int oracle_pfgt(int nd, int dim, double delta, double eps, int iperiod,
     }
     for (b = 0; b < nb; b++) { free(mp[b]); free(loc[b]); }
     free(mp); free(loc); free(W);
+    if (nufft_mode == 1) fast_free(&FN);
   }
   /* step 4: direct, pfgt.f:1082-1136 */
   double dmax = log(1.0 / eps) * delta;
   int ilev;
   for (ilev = 0; ilev <= nlevend; ilev++) {
+#pragma omp parallel for schedule(dynamic) private(i)
     for (b = r->laddr[2 * ilev]; b <= r->laddr[2 * ilev + 1]; b++) {
       int jss = r->isrcse[2 * b], jse = r->isrcse[2 * b + 1];
       int jts = r->itrgse[2 * b], jte = r->itrgse[2 * b + 1];
@@ -1239,6 +1524,13 @@ void oracle_direct_truncated(int nd, int dim, double delta, double dmax, int ns,
   direct_block(nd, dim, delta, dmax, NULL, 0, ns - 1, src, ifcharge, charge, ifdipole,
                rnormal, dipstr, 0, nt - 1, targ, ifpgh, pot, grad, hess);
 }
+
+#ifdef _OPENMP
+#include <omp.h>
+int oracle_threads(void) { return omp_get_max_threads(); }
+#else
+int oracle_threads(void) { return 1; }
+#endif
 
 /* Scalar set-up only (pts_tree_boxsize0 + fgtpwterms) for host-logic tests. */
 void oracle_setup_scalars(int dim, double delta, double eps, int iperiod,

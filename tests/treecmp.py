@@ -10,8 +10,11 @@ def _ids(level, centers):
     return [(int(l), tuple(np.asarray(c, dtype=np.float64).tolist())) for l, c in zip(level, centers)]
 
 
-def compare(gpu, orc, check_lists=True):
-    """Returns a list of mismatch descriptions (empty = identical)."""
+def compare(gpu, orc, check_lists=True, nlevend=None):
+    """Returns a list of mismatch descriptions (empty = identical).
+
+    List 1 is compared for target boxes at levels <= nlevend (the levels the
+    direct loop visits, src/pfgt/pfgt.f:1087)."""
     bad = []
     if gpu["nlevels"] != orc["nlevels"]:
         bad.append(f"nlevels {gpu['nlevels']} != {orc['nlevels']}")
@@ -55,6 +58,8 @@ def compare(gpu, orc, check_lists=True):
     for gi in range(nb):
         k = gid[gi]
         oi = omap[k]
+        if nlevend is not None and k[0] > nlevend:
+            continue
         gs = {gid[s] for s in gpu["l1_src"][gpu["l1_ptr"][gi]:gpu["l1_ptr"][gi + 1]]}
         os_ = {oid[s] for s in orc["list1"][oi, :orc["nlist1"][oi]]}
         if gs != os_:
