@@ -67,11 +67,16 @@ struct Real<float> {
   // exp(-u) for u >= 0 via the hardware base-2 exponential.
   static __device__ __forceinline__ float expm(float u) { return fgt_ex2(-u * 1.4426950408889634f); }
   static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+  static __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
+  // a / b for b in [1, 2] (2 ulp)
+  static __device__ __forceinline__ float div12(float a, float b) { return __fdividef(a, b); }
 };
 template <>
 struct Real<double> {
   static __device__ __forceinline__ double expm(double u) { return exp(-u); }
   static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+  static __device__ __forceinline__ double rsqrt_(double x) { return 1.0 / sqrt(x); }
+  static __device__ __forceinline__ double div12(double a, double b) { return a / b; }
 };
 
 // Morton-style path keys: the digit of level l (child index, bit k set iff

@@ -36,7 +36,7 @@ struct Geo {
 template <typename T>
 struct PWArgs {
   Geo g;
-  T halfw_over_dx, beta, dscale;
+  T halfw_over_dx, inv_hw, beta, dscale;  // inv_hw = dx / halfw
   double scale_d, inv_dx_d, hwdx_d;  // FP64 positions (points are FP64 offsets)
   const T* twf;   // [G][2K+1] fwd full
   const T* twh;   // [G][K+1]  fwd half
@@ -66,47 +66,85 @@ __host__ __device__ constexpr size_t order_offset(int G, int K) {
 template <typename T, int MODE>
 __device__ __forceinline__ void pass_inplace(T* B, int nl, int nb, int SA, int SB, int ein,
                                              int eout, int nin, int nout, const T* __restrict__ tw) {
-  const int lpr = blockDim.x / nout;
-  const int t = threadIdx.x, lo = t / nout, k = t - lo * nout;
-  const bool act_t = lo < lpr;
-  for (int l0 = 0; l0 < nl; l0 += lpr) {
-    const int line = l0 + lo;
-    const bool act = act_t && line < nl;
-    T re = T(0), im = T(0);
-    int base = 0;
-    if (act) {
-      base = (line / nb) * SA + (line % nb) * SB;
+  // register tile: LG lines x KG outputs per thread; a round covers whole
+  // lines (all of a line's inputs are read before any output is written)
+  constexpr int LG = 2, KG = sizeof(T) == 4 ? 4 : 2;
+  const int nkg = (nout + KG - 1) / KG;
+  const int ngroups = blockDim.x / nkg;
+  const int t = threadIdx.x, lg = t / nkg, kg = t - lg * nkg;
+  const bool act_t = lg < ngroups;
+  const int lpr = ngroups * LG;
+  for (int r0 = 0; r0 < nl; r0 += lpr) {
+    T re[LG][KG], im[LG][KG];
+    int base[LG];
+    bool lact[LG];
+#pragma unroll
+    for (int g = 0; g < LG; g++) {
+      const int line = r0 + lg * LG + g;
+      lact[g] = act_t && line < nl;
+      base[g] = lact[g] ? (line / nb) * SA + (line % nb) * SB : 0;
+#pragma unroll
+      for (int j = 0; j < KG; j++) re[g][j] = im[g][j] = T(0);
+    }
+    if (act_t) {
       for (int l = 0; l < nin; l++) {
-        const T twr = tw[2 * (l * nout + k)], twi = tw[2 * (l * nout + k) + 1];
-        if (MODE == 0) {
-          const T gv = B[base + l * ein];
-          re += gv * twr;
-          im += gv * twi;
-        } else {
-          const T xr = B[base + l * ein], xi = B[base + l * ein + 1];
-          re += xr * twr - xi * twi;
-          if (MODE == 1) im += xr * twi + xi * twr;
+        T tr[KG], ti[KG];
+#pragma unroll
+        for (int j = 0; j < KG; j++) {
+          const int k = kg * KG + j;
+          const bool ok = k < nout;
+          tr[j] = ok ? tw[2 * (l * nout + k)] : T(0);
+          ti[j] = ok ? tw[2 * (l * nout + k) + 1] : T(0);
+        }
+#pragma unroll
+        for (int g = 0; g < LG; g++) {
+          if (!lact[g]) continue;
+          if (MODE == 0) {
+            const T gv = B[base[g] + l * ein];
+#pragma unroll
+            for (int j = 0; j < KG; j++) {
+              re[g][j] += gv * tr[j];
+              im[g][j] += gv * ti[j];
+            }
+          } else {
+            const T xr = B[base[g] + l * ein], xi = B[base[g] + l * ein + 1];
+#pragma unroll
+            for (int j = 0; j < KG; j++) {
+              re[g][j] += xr * tr[j] - xi * ti[j];
+              if (MODE == 1) im[g][j] += xr * ti[j] + xi * tr[j];
+            }
+          }
         }
       }
     }
     __syncthreads();
-    if (act) {
-      if (MODE == 2) {
-        B[base + k * eout] = re;
-      } else {
-        B[base + k * eout] = re;
-        B[base + k * eout + 1] = im;
+#pragma unroll
+    for (int g = 0; g < LG; g++) {
+      if (!lact[g]) continue;
+#pragma unroll
+      for (int j = 0; j < KG; j++) {
+        const int k = kg * KG + j;
+        if (k >= nout) break;
+        if (MODE == 2) {
+          B[base[g] + k * eout] = re[g][j];
+        } else {
+          B[base[g] + k * eout] = re[g][j];
+          B[base[g] + k * eout + 1] = im[g][j];
+        }
       }
     }
     __syncthreads();
   }
 }
 
+// ES kernel exp(beta (sqrt(1 - z^2) - 1)) with the exponent written as
+// -beta z^2 / (1 + sqrt(1 - z^2)): no cancellation near the peak, where the
+// direct form loses beta * 2^-24 of relative accuracy in FP32.
 template <typename T>
 __device__ __forceinline__ T es_kernel(T z, T beta) {
-  T u = T(1) - z * z;
-  u = u > T(0) ? u : T(0);
-  return Real<T>::expm(beta * (T(1) - Real<T>::sqrt_(u)));
+  const T q = T(1) - z * z;
+  const T r = q > T(0) ? q * Real<T>::rsqrt_(q) : T(0);
+  return Real<T>::expm(Real<T>::div12(beta * (z * z), T(1) + r));
 }
 
 __device__ __forceinline__ int pmod(int a, int n) {
@@ -114,21 +152,136 @@ __device__ __forceinline__ int pmod(int a, int n) {
   return c < 0 ? c + n : c;
 }
 
+// Stencil cell offsets (T units) along each dimension.  Lin: the sub-grid
+// case, cells base..base+W-1 (offsets fold into address immediates); Tab:
+// the periodic full grid, cells wrap modulo nf (one modulo per dimension).
+// ki[i] for a run-time i without demoting ki to local memory
+__device__ __forceinline__ int sel3(const int* ki, int i) {
+  return i == 0 ? ki[0] : (i == 1 ? ki[1] : ki[2]);
+}
+
 template <int DIM, int W>
-struct CellIdx {
-  int i0[DIM], base[DIM];
-  __device__ __forceinline__ void init(const Geo& g, const int* s) {
+struct LinIdx {
+  int o[DIM];
+  int str0, str1;
+  __device__ __forceinline__ LinIdx(const Geo& g, const int* s) : str0(g.str[0]), str1(g.str[1]) {
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-      i0[d] = s[d];
       int b = s[d] - g.l0;
-      base[d] = b < 0 ? 0 : (b > g.G - W ? g.G - W : b);
+      b = b < 0 ? 0 : (b > g.G - W ? g.G - W : b);
+      o[d] = b * g.str[d];
     }
   }
-  __device__ __forceinline__ int at(const Geo& g, int d, int j) const {
-    return g.wrap ? pmod(i0[d] + j, g.nf) : base[d] + j;
-  }
+  __device__ __forceinline__ int x(int j) const { return o[0] + j * (DIM == 1 ? 1 : str0); }
+  __device__ __forceinline__ int y(int j) const { return o[1] + j * (DIM == 2 ? 1 : str1); }
+  __device__ __forceinline__ int z(int j) const { return o[DIM - 1] + j; }
 };
+template <int DIM, int W>
+struct TabIdx {
+  int o[DIM][W];
+  __device__ __forceinline__ TabIdx(const Geo& g, const int* s) {
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      int c = pmod(s[d], g.nf);
+#pragma unroll
+      for (int j = 0; j < W; j++) {
+        o[d][j] = c * g.str[d];
+        c = c + 1 == g.nf ? 0 : c + 1;
+      }
+    }
+  }
+  __device__ __forceinline__ int x(int j) const { return o[0][j]; }
+  __device__ __forceinline__ int y(int j) const { return o[1][j]; }
+  __device__ __forceinline__ int z(int j) const { return o[DIM - 1][j]; }
+};
+
+// Calls body(x offset, weight) for the W cells of a stencil's outer dimension
+// with every register-array index a compile-time constant, so the kernel
+// values never go to local memory: fully unrolled for W <= U, otherwise a
+// rolled loop over rotating registers.
+template <typename T, int W, int U, class IX, class F>
+__device__ __forceinline__ void outer_cells(const IX& ix, const T* ph0, F&& body) {
+  if constexpr (W <= U) {
+#pragma unroll
+    for (int j = 0; j < W; j++) body(ix.x(j), ph0[j]);
+  } else {
+    int xo[W];
+    T pw[W];
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+      xo[j] = ix.x(j);
+      pw[j] = ph0[j];
+    }
+#pragma unroll 1
+    for (int j = 0; j < W; j++) {
+      body(xo[0], pw[0]);
+#pragma unroll
+      for (int k = 0; k + 1 < W; k++) {
+        xo[k] = xo[k + 1];
+        pw[k] = pw[k + 1];
+      }
+    }
+  }
+}
+
+template <typename T, int DIM, int W, class IX>
+__device__ __forceinline__ T interp_cells(const T* B, const IX& ix, const T (*ph)[W]) {
+  T acc = T(0);
+  if constexpr (DIM == 1) {
+#pragma unroll
+    for (int j = 0; j < W; j++) acc += B[ix.x(j)] * ph[0][j];
+  } else if constexpr (DIM == 2) {
+    outer_cells<T, W, 16>(ix, ph[0], [&](int xo, T p0) {
+      const T* bx = B + xo;
+      T sy = T(0);
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) sy += bx[ix.z(jy)] * ph[1][jy];
+      acc += sy * p0;
+    });
+  } else {
+    outer_cells<T, W, 8>(ix, ph[0], [&](int xo, T p0) {
+      const T* bx = B + xo;
+      T sx = T(0);
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        const T* bxy = bx + ix.y(jy);
+        T sy = T(0);
+#pragma unroll
+        for (int jz = 0; jz < W; jz++) sy += bxy[ix.z(jz)] * ph[2][jz];
+        sx += sy * ph[1][jy];
+      }
+      acc += sx * p0;
+    });
+  }
+  return acc;
+}
+
+template <typename T, int DIM, int W, class IX>
+__device__ __forceinline__ void spread_cells(T* B, const IX& ix, const T (*ph)[W], T str) {
+  if constexpr (DIM == 1) {
+#pragma unroll
+    for (int j = 0; j < W; j++) atomicAdd(B + ix.x(j), str * ph[0][j]);
+  } else if constexpr (DIM == 2) {
+    outer_cells<T, W, 16>(ix, ph[0], [&](int xo, T p0) {
+      T* bx = B + xo;
+      const T v = str * p0;
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) atomicAdd(bx + ix.z(jy), v * ph[1][jy]);
+    });
+  } else {
+    outer_cells<T, W, 8>(ix, ph[0], [&](int xo, T p0) {
+      T* bx = B + xo;
+      const T vx = str * p0;
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        T* bxy = bx + ix.y(jy);
+        const T vxy = vx * ph[1][jy];
+#pragma unroll
+        for (int jz = 0; jz < W; jz++) atomicAdd(bxy + ix.z(jz), vxy * ph[2][jz]);
+      }
+    });
+  }
+}
 
 // Thread-per-point interpolation (component grids of the hessian path).
 template <typename T, int W>
@@ -137,85 +290,171 @@ __device__ __forceinline__ int kernel_row(const PWArgs<T>& a, double x, T* phi) 
   const int i0 = (int)ceil(u - a.hwdx_d);
   const T f0 = (T)((double)i0 - u);
 #pragma unroll
-  for (int j = 0; j < W; j++) phi[j] = es_kernel<T>((f0 + (T)j) / a.halfw_over_dx, a.beta);
+  for (int j = 0; j < W; j++) phi[j] = es_kernel<T>((f0 + (T)j) * a.inv_hw, a.beta);
   return i0;
 }
 
 template <typename T, int DIM, int W>
 __device__ __forceinline__ T interp_point(const PWArgs<T>& a, const T* B, const double* x) {
-  const Geo& g = a.g;
   T ph[DIM][W];
   int s[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; d++) s[d] = kernel_row<T, W>(a, x[d], ph[d]);
-  CellIdx<DIM, W> c;
-  c.init(g, s);
-  T acc = T(0);
-  if (DIM == 1) {
-#pragma unroll
-    for (int j = 0; j < W; j++) acc += B[c.at(g, 0, j)] * ph[0][j];
-  } else if (DIM == 2) {
-#pragma unroll 1
-    for (int jx = 0; jx < W; jx++) {
-      const int bx = c.at(g, 0, jx) * g.str[0];
-      T sy = T(0);
-#pragma unroll
-      for (int jy = 0; jy < W; jy++) sy += B[bx + c.at(g, 1, jy)] * ph[1][jy];
-      acc += sy * ph[0][jx];
-    }
-  } else {
-#pragma unroll 1
-    for (int jx = 0; jx < W; jx++) {
-      const int bx = c.at(g, 0, jx) * g.str[0];
-      T sx = T(0);
-#pragma unroll
-      for (int jy = 0; jy < W; jy++) {
-        const int bxy = bx + c.at(g, 1, jy) * g.str[1];
-        T sy = T(0);
-#pragma unroll
-        for (int jz = 0; jz < W; jz++) sy += B[bxy + c.at(g, 2, jz)] * ph[2][jz];
-        sx += sy * ph[1][jy];
-      }
-      acc += sx * ph[0][jx];
-    }
-  }
-  return acc;
+  if (a.g.wrap) return interp_cells<T, DIM, W>(B, TabIdx<DIM, W>(a.g, s), ph);
+  return interp_cells<T, DIM, W>(B, LinIdx<DIM, W>(a.g, s), ph);
 }
 
 template <typename T, int DIM, int W>
 __device__ __forceinline__ void spread_point(const PWArgs<T>& a, T* B, const double* x, T str) {
-  const Geo& g = a.g;
   T ph[DIM][W];
   int s[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; d++) s[d] = kernel_row<T, W>(a, x[d], ph[d]);
-  CellIdx<DIM, W> c;
-  c.init(g, s);
-  if (DIM == 1) {
+  if (a.g.wrap)
+    spread_cells<T, DIM, W>(B, TabIdx<DIM, W>(a.g, s), ph, str);
+  else
+    spread_cells<T, DIM, W>(B, LinIdx<DIM, W>(a.g, s), ph, str);
+}
+
+// Kernel values and their derivatives with respect to the point's original
+// coordinate: d/dx phi((x_c - x)/halfw) = phi * beta * z / (sqrt(1-z^2) halfw),
+// times the coordinate scale (a.dscale = scale / halfw).  Zero at |z| = 1.
+template <typename T, int W>
+__device__ __forceinline__ int kernel_row_d(const PWArgs<T>& a, double x, T* phi, T* dphi) {
+  const double u = x * a.inv_dx_d;
+  const int i0 = (int)ceil(u - a.hwdx_d);
+  const T f0 = (T)((double)i0 - u);
 #pragma unroll
-    for (int j = 0; j < W; j++) atomicAdd(&B[c.at(g, 0, j)], str * ph[0][j]);
-  } else if (DIM == 2) {
-#pragma unroll 1
-    for (int jx = 0; jx < W; jx++) {
-      const int bx = c.at(g, 0, jx) * g.str[0];
-      const T v = str * ph[0][jx];
+  for (int j = 0; j < W; j++) {
+    const T z = (f0 + (T)j) * a.inv_hw;
+    const T q = T(1) - z * z;
+    const T rq = q > T(0) ? Real<T>::rsqrt_(q) : T(0);
+    const T e = Real<T>::expm(Real<T>::div12(a.beta * (z * z), T(1) + q * rq));
+    phi[j] = e;
+    dphi[j] = e * (a.beta * a.dscale) * z * rq;
+  }
+  return i0;
+}
+
+// outer_cells with a second weight row (value and derivative along x)
+template <typename T, int W, int U, class IX, class F>
+__device__ __forceinline__ void outer_cells2(const IX& ix, const T* p0, const T* q0, F&& body) {
+  if constexpr (W <= U) {
 #pragma unroll
-      for (int jy = 0; jy < W; jy++) atomicAdd(&B[bx + c.at(g, 1, jy)], v * ph[1][jy]);
-    }
+    for (int j = 0; j < W; j++) body(ix.x(j), p0[j], q0[j]);
   } else {
+    int xo[W];
+    T pw[W], qw[W];
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+      xo[j] = ix.x(j);
+      pw[j] = p0[j];
+      qw[j] = q0[j];
+    }
 #pragma unroll 1
-    for (int jx = 0; jx < W; jx++) {
-      const int bx = c.at(g, 0, jx) * g.str[0];
-      const T vx = str * ph[0][jx];
+    for (int j = 0; j < W; j++) {
+      body(xo[0], pw[0], qw[0]);
 #pragma unroll
-      for (int jy = 0; jy < W; jy++) {
-        const int bxy = bx + c.at(g, 1, jy) * g.str[1];
-        const T vxy = vx * ph[1][jy];
-#pragma unroll
-        for (int jz = 0; jz < W; jz++) atomicAdd(&B[bxy + c.at(g, 2, jz)], vxy * ph[2][jz]);
+      for (int k = 0; k + 1 < W; k++) {
+        xo[k] = xo[k + 1];
+        pw[k] = pw[k + 1];
+        qw[k] = qw[k + 1];
       }
     }
   }
+}
+
+// Potential and gradient of one grid at one point: v[0] = pot, v[1+d] = d/dx_d.
+// The sums run over B - Bref (Bref = the stencil's centre cell): the
+// derivative stencils sum to the derivative of the kernel's partition of
+// unity, which is at the aliasing level, so dropping Bref from them changes
+// nothing, while the smaller summands keep the FP32 sums from cancelling
+// when the field varies slowly over the stencil.  The potential adds Bref
+// times the product of the kernel row sums back.
+template <typename T, int DIM, int W, class IX>
+__device__ __forceinline__ void interp_grad_cells(const T* B, const IX& ix, const T (*ph)[W],
+                                                  const T (*dph)[W], T* v) {
+  T ksum = T(1);
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    T sd = T(0);
+#pragma unroll
+    for (int j = 0; j < W; j++) sd += ph[d][j];
+    ksum *= sd;
+  }
+  if constexpr (DIM == 1) {
+    const T bref = B[ix.x(W / 2)];
+    T s0 = T(0), s1 = T(0);
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+      const T b = B[ix.x(j)] - bref;
+      s0 += b * ph[0][j];
+      s1 += b * dph[0][j];
+    }
+    v[0] = s0 + bref * ksum;
+    v[1] = s1;
+  } else if constexpr (DIM == 2) {
+    const T bref = B[ix.x(W / 2) + ix.z(W / 2)];
+    T pot = T(0), gx = T(0), gy = T(0);
+    outer_cells2<T, W, 16>(ix, ph[0], dph[0], [&](int xo, T px, T dpx) {
+      const T* bx = B + xo;
+      T s0 = T(0), s1 = T(0);
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        const T b = bx[ix.z(jy)] - bref;
+        s0 += b * ph[1][jy];
+        s1 += b * dph[1][jy];
+      }
+      pot += px * s0;
+      gx += dpx * s0;
+      gy += px * s1;
+    });
+    v[0] = pot + bref * ksum;
+    v[1] = gx;
+    v[2] = gy;
+  } else {
+    const T bref = B[ix.x(W / 2) + ix.y(W / 2) + ix.z(W / 2)];
+    T pot = T(0), gx = T(0), gy = T(0), gz = T(0);
+    outer_cells2<T, W, 8>(ix, ph[0], dph[0], [&](int xo, T px, T dpx) {
+      const T* bx = B + xo;
+      T t0 = T(0), t1 = T(0), t2 = T(0);
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        const T* bxy = bx + ix.y(jy);
+        T s0 = T(0), s1 = T(0);
+#pragma unroll
+        for (int jz = 0; jz < W; jz++) {
+          const T b = bxy[ix.z(jz)] - bref;
+          s0 += b * ph[2][jz];
+          s1 += b * dph[2][jz];
+        }
+        t0 += ph[1][jy] * s0;
+        t1 += dph[1][jy] * s0;
+        t2 += ph[1][jy] * s1;
+      }
+      pot += px * t0;
+      gx += dpx * t0;
+      gy += px * t1;
+      gz += px * t2;
+    });
+    v[0] = pot + bref * ksum;
+    v[1] = gx;
+    v[2] = gy;
+    v[3] = gz;
+  }
+}
+
+template <typename T, int DIM, int W>
+__device__ __forceinline__ void interp_grad_point(const PWArgs<T>& a, const T* B, const double* x,
+                                                  T* v) {
+  T ph[DIM][W], dph[DIM][W];
+  int s[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) s[d] = kernel_row_d<T, W>(a, x[d], ph[d], dph[d]);
+  if (a.g.wrap)
+    interp_grad_cells<T, DIM, W>(B, TabIdx<DIM, W>(a.g, s), ph, dph, v);
+  else
+    interp_grad_cells<T, DIM, W>(B, LinIdx<DIM, W>(a.g, s), ph, dph, v);
 }
 
 // Bank-balanced processing order of a chunk of points.  Thread-per-point
@@ -278,7 +517,172 @@ struct FormPtrs {
   T* mp;                 // [n_form][nd][nexp] complex
 };
 
-template <typename T, int DIM, int W, bool GB>
+// ------------------------------------------------ block-tiled spreading (3D)
+// The box's points are counting-sorted by 4x4x4 block of stencil base cells.
+// A warp takes one block at a time and accumulates all of its points into a
+// register tile of (4+W-1)^3 cells: lane l owns the tile columns (tx,ty) =
+// l, l+32, ... with all TILE z cells.  Per point the warp reads the point's
+// three shifted kernel rows (zero outside the stencil) from shared memory and
+// does NCOL*TILE FMAs per lane; the tile is flushed once per block with one
+// shared-memory atomic per non-zero cell, instead of W^3 atomics per point.
+constexpr int TB = 4;           // block edge (base cells)
+constexpr int NBLK_MAX = 1024;  // blocks per box
+constexpr int FCH = 8192;       // points sorted per round
+constexpr int PB = 8;           // points per warp batch
+constexpr int TP = 12;          // padded kernel row (TILE <= TP - 1)
+
+template <typename T>
+__host__ __device__ constexpr size_t tiled_offset(int G, int K) {
+  return ((size_t)sizeof(T) * 2 * G * ((2 * K + 1) + (K + 1)) + sizeof(int) * (2 * NBLK_MAX + 32) +
+          sizeof(int) * FCH + sizeof(unsigned short) * FCH +
+          sizeof(float) * (PW_THREADS / 32) * PB * 3 * TP + 15) &
+         ~(size_t)15;
+}
+
+// Exclusive scan of cnt[0..n) into off[0..n) for n <= 2 * blockDim.x;
+// ws holds blockDim.x / 32 ints.  Ends with a block barrier.
+__device__ __forceinline__ void block_scan(const int* cnt, int* off, int n, int* ws) {
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5, nw = blockDim.x >> 5;
+  const int v0 = 2 * t < n ? cnt[2 * t] : 0, v1 = 2 * t + 1 < n ? cnt[2 * t + 1] : 0;
+  const int s = v0 + v1;
+  int inc = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += u;
+  }
+  if (lane == 31) ws[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    const int x = lane < nw ? ws[lane] : 0;
+    int ix = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, ix, o);
+      if (lane >= o) ix += u;
+    }
+    if (lane < nw) ws[lane] = ix - x;
+  }
+  __syncthreads();
+  const int ex = ws[w] + inc - s;
+  if (2 * t < n) off[2 * t] = ex;
+  if (2 * t + 1 < n) off[2 * t + 1] = ex + v0;
+  __syncthreads();
+}
+
+template <typename T, int W>
+__device__ __forceinline__ int base_cell(const PWArgs<T>& a, double xs) {
+  const double u = xs * a.inv_dx_d;
+  const int b = (int)ceil(u - a.hwdx_d) - a.g.l0;
+  return b < 0 ? 0 : (b > a.g.G - W ? a.g.G - W : b);
+}
+
+// Spread points c0..c0+n-1 (n <= FCH) of one strength set into B.
+// sq: charges (is_q) or dipole strengths, sr: dipole direction component.
+template <typename T, int W>
+__device__ void spread_tiled(const PWArgs<T>& a, T* B, const double* __restrict__ off, int ns,
+                             const T* __restrict__ sq, const T* __restrict__ sr, bool is_q, int c0,
+                             int n, int* cnt, int* boff, int* misc, int* tmp,
+                             unsigned short* perm, T* rows) {
+  constexpr int TILE = TB + W - 1, NCOL = (TILE * TILE + 31) / 32;
+  static_assert(TILE <= TP - 1, "tile row too long");
+  const Geo& g = a.g;
+  const int nbd = (g.G - W + 1 + TB - 1) / TB, nblk = nbd * nbd * nbd;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) cnt[i] = 0;
+  if (threadIdx.x == 0) misc[0] = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int blk = 0;
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      blk = blk * nbd + base_cell<T, W>(a, off[(size_t)d * ns + c0 + i] * a.scale_d) / TB;
+    const int r = atomicAdd(&cnt[blk], 1);
+    tmp[i] = (r << 10) | blk;
+  }
+  __syncthreads();
+  block_scan(cnt, boff, nblk, misc + 1);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int v = tmp[i];
+    perm[boff[v & (NBLK_MAX - 1)] + (v >> 10)] = (unsigned short)i;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T* R = rows + warp * (PB * 3 * TP);
+  int cx[NCOL], cy[NCOL];  // slots past the tile read the zero entry TP-1
+#pragma unroll
+  for (int j = 0; j < NCOL; j++) {
+    const int c = lane + 32 * j;
+    cx[j] = c < TILE * TILE ? c / TILE : TP - 1;
+    cy[j] = c < TILE * TILE ? c % TILE : TP - 1;
+  }
+  for (;;) {
+    int bi = 0;
+    if (lane == 0) bi = atomicAdd(&misc[0], 1);
+    bi = __shfl_sync(0xffffffffu, bi, 0);
+    if (bi >= nblk) break;
+    const int nb = cnt[bi];
+    if (nb == 0) continue;
+    const int start = boff[bi];
+    int org[3];
+    org[2] = (bi % nbd) * TB;
+    org[1] = ((bi / nbd) % nbd) * TB;
+    org[0] = (bi / (nbd * nbd)) * TB;
+    T acc[NCOL][TILE];
+#pragma unroll
+    for (int j = 0; j < NCOL; j++)
+#pragma unroll
+      for (int t = 0; t < TILE; t++) acc[j][t] = T(0);
+    for (int k0 = 0; k0 < nb; k0 += PB) {
+      const int np = min(PB, nb - k0);
+      if (lane < 3 * PB) {
+        const int pp = lane % PB, d = lane / PB;
+        if (pp < np) {
+          T* row = R + (pp * 3 + d) * TP;
+          const int pt = c0 + perm[start + k0 + pp];
+          T ph[W];
+          const double x = off[(size_t)d * ns + pt] * a.scale_d;
+          const int i0 = kernel_row<T, W>(a, x, ph);
+          int b = i0 - g.l0;
+          b = b < 0 ? 0 : (b > g.G - W ? g.G - W : b);
+          const int o = b - org[d];
+          const T sc = d == 0 ? (is_q ? sq[pt] : sq[pt] * sr[pt]) : T(1);
+#pragma unroll
+          for (int t = 0; t < TP; t++) row[t] = T(0);
+#pragma unroll
+          for (int j = 0; j < W; j++) row[o + j] = ph[j] * sc;
+        }
+      }
+      __syncwarp();
+#pragma unroll 1
+      for (int pq = 0; pq < np; pq++) {
+        const T* row = R + pq * 3 * TP;
+        T rz[TP];
+#pragma unroll
+        for (int t = 0; t < TP; t++) rz[t] = row[2 * TP + t];
+#pragma unroll
+        for (int j = 0; j < NCOL; j++) {
+          const T v = row[cx[j]] * row[TP + cy[j]];
+#pragma unroll
+          for (int t = 0; t < TILE; t++) acc[j][t] = fma(v, rz[t], acc[j][t]);
+        }
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int j = 0; j < NCOL; j++) {
+      const int x = org[0] + cx[j], y = org[1] + cy[j];
+      if (lane + 32 * j < TILE * TILE && x < g.G && y < g.G) {
+        T* col = B + x * g.str[0] + y * g.str[1] + org[2];
+#pragma unroll
+        for (int t = 0; t < TILE; t++)
+          if (org[2] + t < g.G && acc[j][t] != T(0)) atomicAdd(col + t, acc[j][t]);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <typename T, int DIM, int W, bool GB, bool TILED>
 __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, FormPtrs<T> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geo& g = a.g;
@@ -286,11 +690,20 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
   T* sm = reinterpret_cast<T*>(smem_raw);
   T* twf = sm;                // G*NF complex
   T* twh = twf + 2 * G * NF;  // G*NH complex
+  // atomic-spreading scratch
   int* ordtmp = reinterpret_cast<int*>(twh + 2 * G * NH);  // ORDER_CHUNK
   int* ordcnt = ordtmp + ORDER_CHUNK;                        // 32
   unsigned short* perm = reinterpret_cast<unsigned short*>(ordcnt + 32);  // ORDER_CHUNK
+  // tiled-spreading scratch
+  int* tcnt = reinterpret_cast<int*>(twh + 2 * G * NH);  // NBLK_MAX
+  int* toff = tcnt + NBLK_MAX;                             // NBLK_MAX
+  int* tmisc = toff + NBLK_MAX;                            // 32
+  int* ttmp = tmisc + 32;                                  // FCH
+  unsigned short* tperm = reinterpret_cast<unsigned short*>(ttmp + FCH);  // FCH
+  T* trows = reinterpret_cast<T*>(tperm + FCH);  // warps * PB * 3 * TP
   T* B = GB ? a.gscratch + (size_t)blockIdx.x * g.bufsz
-            : reinterpret_cast<T*>(smem_raw + order_offset<T>(G, K));
+            : reinterpret_cast<T*>(smem_raw + (TILED ? tiled_offset<T>(G, K)
+                                                     : order_offset<T>(G, K)));
   load_tw(twf, a.twf, 2 * G * NF);
   load_tw(twh, a.twh, 2 * G * NH);
   __syncthreads();
@@ -306,19 +719,27 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
         const int dd = is_q ? -1 : comp - io.has_q;
         for (int i = threadIdx.x; i < g.bufsz; i += blockDim.x) B[i] = T(0);
         __syncthreads();
-        for (int c0 = p0; c0 < p1; c0 += ORDER_CHUNK) {
-          const int n = min(ORDER_CHUNK, p1 - c0);
-          order_chunk<T, DIM, W>(a, p.off, io.ns, c0, n, perm, ordtmp, ordcnt);
-          for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int pt = c0 + perm[i];
-            double x[DIM];
+        if constexpr (TILED) {
+          const T* sq = is_q ? p.q + (size_t)id * io.ns : p.ds + (size_t)id * io.ns;
+          const T* sr = is_q ? nullptr : p.rn + (size_t)dd * io.ns;
+          for (int c0 = p0; c0 < p1; c0 += FCH)
+            spread_tiled<T, W>(a, B, p.off, io.ns, sq, sr, is_q, c0, min(FCH, p1 - c0), tcnt, toff,
+                               tmisc, ttmp, tperm, trows);
+        } else {
+          for (int c0 = p0; c0 < p1; c0 += ORDER_CHUNK) {
+            const int n = min(ORDER_CHUNK, p1 - c0);
+            order_chunk<T, DIM, W>(a, p.off, io.ns, c0, n, perm, ordtmp, ordcnt);
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+              const int pt = c0 + perm[i];
+              double x[DIM];
 #pragma unroll
-            for (int k = 0; k < DIM; k++) x[k] = p.off[(size_t)k * io.ns + pt] * a.scale_d;
-            const T str = is_q ? p.q[(size_t)id * io.ns + pt]
-                               : p.ds[(size_t)id * io.ns + pt] * p.rn[(size_t)dd * io.ns + pt];
-            spread_point<T, DIM, W>(a, B, x, str);
+              for (int k = 0; k < DIM; k++) x[k] = p.off[(size_t)k * io.ns + pt] * a.scale_d;
+              const T str = is_q ? p.q[(size_t)id * io.ns + pt]
+                                 : p.ds[(size_t)id * io.ns + pt] * p.rn[(size_t)dd * io.ns + pt];
+              spread_point<T, DIM, W>(a, B, x, str);
+            }
+            __syncthreads();
           }
-          __syncthreads();
         }
         // passes on the last and middle dimensions
         if (DIM == 3) {
@@ -367,7 +788,7 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
           for (int d = 0; d < DIM; d++) f *= a.facf[ki[d]];
           T vr = re * f, vi = im * f;
           if (!is_q) {  // * (-i) ts(k_d) / sqrt(delta0)
-            const T cc = a.ts[ki[dd]] * a.inv_sqd0;
+            const T cc = a.ts[sel3(ki, dd)] * a.inv_sqd0;
             const T tr = vi * cc, ti = -vr * cc;
             vr = tr;
             vi = ti;
@@ -469,14 +890,14 @@ __device__ __forceinline__ void eval_factor(const PWArgs<T>& a, int c, const int
   }
   if (c <= DIM) {  // i ts(k_d)/sqrt(delta0)
     fr = T(0);
-    fi = a.ts[ki[c - 1]] * a.inv_sqd0;
+    fi = a.ts[sel3(ki, c - 1)] * a.inv_sqd0;
     return;
   }
   int m = c - 1 - DIM, p, q;
   if (DIM == 1) { p = 0; q = 0; }
   else if (DIM == 2) { p = (m == 2) ? 1 : 0; q = (m == 0) ? 0 : 1; }
   else { p = m < 3 ? m : (m < 5 ? 0 : 1); q = m < 3 ? m : (m == 3 ? 1 : 2); }
-  fr = -a.ts[ki[p]] * a.ts[ki[q]] * a.inv_sqd0 * a.inv_sqd0;
+  fr = -a.ts[sel3(ki, p)] * a.ts[sel3(ki, q)] * a.inv_sqd0 * a.inv_sqd0;
   fi = T(0);
 }
 
@@ -491,7 +912,7 @@ __device__ __forceinline__ void build_eval_grid(const PWArgs<T>& a, const T* L, 
     for (int l = threadIdx.x; l < G; l += blockDim.x) {
       T acc = T(0);
       for (int k = 0; k < NH; k++) {
-        int ki[1] = {k + K};
+        int ki[3] = {k + K, 0, 0};
         T fr, fi;
         eval_factor<T, DIM>(a, c, ki, fr, fi);
         const T f = a.faci[k + K];
@@ -542,9 +963,11 @@ __device__ __forceinline__ void build_eval_grid(const PWArgs<T>& a, const T* L, 
   }
 }
 
-// One grid per output component (pot, grad_k, hess_kl) and thread-per-point
-// interpolation of both evaluation sets in bank-balanced order.
-template <typename T, int DIM, int W, bool GB>
+// Thread-per-point interpolation of both evaluation sets in bank-balanced
+// order.  DERIV: one potential grid, gradients through the kernel derivative
+// (no hessians); otherwise one grid per output component (pot, grad_k,
+// hess_kl).
+template <typename T, int DIM, int W, bool GB, bool DERIV>
 __global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<T> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geo& g = a.g;
@@ -565,21 +988,39 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<
     const int box = p.eval_box[e];
     for (int id = 0; id < p.nd; id++) {
       const T* L = p.loc + ((size_t)e * p.nd + id) * 2 * g.nexp;
-      for (int c = 0; c < p.ncomp_max; c++) {
+      for (int c = 0; c < (DERIV ? 1 : p.ncomp_max); c++) {
         build_eval_grid<T, DIM>(a, L, c, B, tif, tih);
         for (int set = 0; set < 2; set++) {
-          if (c >= p.ncomp[set] || p.n[set] == 0) continue;
-          const int q0 = p.lo[set][box], q1 = p.hi[set][box], ne = p.n[set];
+          // select by value: indexing the parameter arrays with a run-time
+          // index would copy them to local memory
+          const int ne = set ? p.n[1] : p.n[0];
+          if (c >= (set ? p.ncomp[1] : p.ncomp[0]) || ne == 0) continue;
+          const double* offs = set ? p.off[1] : p.off[0];
+          double* outs = set ? p.out[1] : p.out[0];
+          const int q0 = set ? p.lo[1][box] : p.lo[0][box];
+          const int q1 = set ? p.hi[1][box] : p.hi[0][box];
           for (int c0 = q0; c0 < q1; c0 += ORDER_CHUNK) {
             const int n = min(ORDER_CHUNK, q1 - c0);
-            order_chunk<T, DIM, W>(a, p.off[set], ne, c0, n, perm, ordtmp, ordcnt);
+            order_chunk<T, DIM, W>(a, offs, ne, c0, n, perm, ordtmp, ordcnt);
             for (int i = threadIdx.x; i < n; i += blockDim.x) {
               const int pt = c0 + perm[i];
               double x[DIM];
 #pragma unroll
-              for (int k = 0; k < DIM; k++) x[k] = p.off[set][(size_t)k * ne + pt] * a.scale_d;
-              const T v = interp_point<T, DIM, W>(a, B, x);
-              p.out[set][((size_t)c * p.nd + id) * ne + pt] += (double)v;
+              for (int k = 0; k < DIM; k++) x[k] = offs[(size_t)k * ne + pt] * a.scale_d;
+              if constexpr (DERIV) {
+                T v[1 + DIM];
+                interp_grad_point<T, DIM, W>(a, B, x, v);
+                const int nc = set ? p.ncomp[1] : p.ncomp[0];
+                outs[(size_t)id * ne + pt] += (double)v[0];
+                if (nc > 1) {
+#pragma unroll
+                  for (int d = 0; d < DIM; d++)
+                    outs[((size_t)(1 + d) * p.nd + id) * ne + pt] += (double)v[1 + d];
+                }
+              } else {
+                const T v = interp_point<T, DIM, W>(a, B, x);
+                outs[((size_t)c * p.nd + id) * ne + pt] += (double)v;
+              }
             }
             __syncthreads();
           }
@@ -603,13 +1044,17 @@ __global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal(PWArgs<T> a, EvalP
     const int e = p.boxes[bi];
     const int box = p.eval_box[e];
     for (int set = 0; set < 2; set++) {
-      if (p.n[set] == 0 || p.ncomp[set] == 0) continue;
-      const int q0 = p.lo[set][box], q1 = p.hi[set][box], ne = p.n[set], nc = p.ncomp[set];
+      const int ne = set ? p.n[1] : p.n[0], nc = set ? p.ncomp[1] : p.ncomp[0];
+      if (ne == 0 || nc == 0) continue;
+      const double* offs = set ? p.off[1] : p.off[0];
+      double* outs = set ? p.out[1] : p.out[0];
+      const int q0 = set ? p.lo[1][box] : p.lo[0][box];
+      const int q1 = set ? p.hi[1][box] : p.hi[0][box];
       for (int pt = q0; pt < q1; pt++) {
         __syncthreads();
         for (int i = threadIdx.x; i < DIM * NF; i += blockDim.x) {
           const int d = i / NF, k = i - d * NF - K;
-          const double x = p.off[set][(size_t)d * ne + pt] * a.scale_d;
+          const double x = offs[(size_t)d * ne + pt] * a.scale_d;
           double sn, cs;
           sincos(x * (double)k, &sn, &cs);
           E[2 * i] = (T)cs;
@@ -649,7 +1094,7 @@ __global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal(PWArgs<T> a, EvalP
                 if (DIM == 1) { pp = 0; qq = 0; }
                 else if (DIM == 2) { pp = (hm == 2) ? 1 : 0; qq = (hm == 0) ? 0 : 1; }
                 else { pp = hm < 3 ? hm : (hm < 5 ? 0 : 1); qq = hm < 3 ? hm : (hm == 3 ? 1 : 2); }
-                acc[1 + DIM + hm] += -tr * a.ts[ki[pp]] * a.ts[ki[qq]] * a.inv_sqd0 * a.inv_sqd0;
+                acc[1 + DIM + hm] += -tr * a.ts[sel3(ki, pp)] * a.ts[sel3(ki, qq)] * a.inv_sqd0 * a.inv_sqd0;
               }
             }
           }
@@ -663,7 +1108,7 @@ __global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal(PWArgs<T> a, EvalP
           if (threadIdx.x < nc) {
             double v = 0;
             for (int j = 0; j < (int)(blockDim.x >> 5); j++) v += red[j][threadIdx.x];
-            p.out[set][((size_t)threadIdx.x * p.nd + id) * ne + pt] += v;
+            outs[((size_t)threadIdx.x * p.nd + id) * ne + pt] += v;
           }
           __syncthreads();
         }
@@ -748,6 +1193,7 @@ void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s
   a.inv_dx_d = 1.0 / P.dx;
   a.hwdx_d = P.halfw / P.dx;
   a.halfw_over_dx = (T)(P.halfw / P.dx);
+  a.inv_hw = (T)(P.dx / P.halfw);
   a.beta = (T)P.beta;
   a.dscale = (T)(a.inv_dx_d * a.scale_d / a.hwdx_d);
   a.inv_sqd0 = (T)(1.0 / P.sqd0);
@@ -812,14 +1258,25 @@ int launch_form(PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>& 
   size_t fix = fixed_smem(a, W, 1);
   size_t need = fix + sizeof(T) * (size_t)a.g.bufsz;
   int grid = std::max(1, std::min(io.n_form, kSMs));
+  if constexpr (std::is_same<T, float>::value && DIM == 3 && TB + W - 1 <= TP - 1) {
+    const int nbd = (a.g.G - W + 1 + TB - 1) / TB;
+    const size_t tneed = tiled_offset<T>(a.g.G, a.g.K) + sizeof(T) * (size_t)a.g.bufsz;
+    if (!a.g.wrap && nbd * nbd * nbd <= NBLK_MAX && tneed <= (size_t)MAXSMEM) {
+      auto k = k_form<T, DIM, W, false, true>;
+      set_smem(k, tneed);
+      k<<<grid, PW_THREADS, tneed, s>>>(a, io, fp);
+      FGT_LAUNCH_CHECK();
+      return 1;
+    }
+  }
   if (need <= (size_t)MAXSMEM) {
-    auto k = k_form<T, DIM, W, false>;
+    auto k = k_form<T, DIM, W, false, false>;
     set_smem(k, need);
     k<<<grid, PW_THREADS, need, s>>>(a, io, fp);
   } else {
     gs.alloc((size_t)grid * a.g.bufsz, s);
     a.gscratch = gs;
-    auto k = k_form<T, DIM, W, true>;
+    auto k = k_form<T, DIM, W, true, false>;
     set_smem(k, fix);
     k<<<grid, PW_THREADS, fix, s>>>(a, io, fp);
   }
@@ -827,8 +1284,8 @@ int launch_form(PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>& 
   return 1;
 }
 
-template <typename T, int DIM, int W>
-int launch_eval(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t s) {
+template <typename T, int DIM, int W, bool DERIV>
+int launch_eval_k(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t s) {
   size_t fix = fixed_smem(a, W, 2);
   size_t need = fix + sizeof(T) * (size_t)a.g.bufsz;
   int grid = std::max(1, std::min(ep.nbox, kSMs));
@@ -839,16 +1296,26 @@ int launch_eval(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t s
   }
   size_t sm = gb ? fix : need;
   if (gb) {
-    auto k = k_eval_comp<T, DIM, W, true>;
+    auto k = k_eval_comp<T, DIM, W, true, DERIV>;
     set_smem(k, sm);
     k<<<grid, PW_THREADS, sm, s>>>(a, ep);
   } else {
-    auto k = k_eval_comp<T, DIM, W, false>;
+    auto k = k_eval_comp<T, DIM, W, false, DERIV>;
     set_smem(k, sm);
     k<<<grid, PW_THREADS, sm, s>>>(a, ep);
   }
   FGT_LAUNCH_CHECK();
   return 1;
+}
+
+// deriv: gradients through the kernel derivative (widths 8..16 only)
+template <typename T, int DIM, int W>
+int launch_eval(PWArgs<T>& a, const EvalPtrs<T>& ep, bool deriv, DBuf<T>& gs, cudaStream_t s) {
+  if constexpr (W >= 8) {
+    if (deriv) return launch_eval_k<T, DIM, W, true>(a, ep, gs, s);
+  }
+  FGT_REQUIRE(!deriv, FGT_ERR_UNSUPPORTED, "derivative evaluation needs a kernel width >= 8");
+  return launch_eval_k<T, DIM, W, false>(a, ep, gs, s);
 }
 
 template <typename T, int DIM>
@@ -863,21 +1330,22 @@ int form_w(int w, PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>
   }
 }
 template <typename T, int DIM>
-int eval_w(int w, PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t s) {
+int eval_w(int w, PWArgs<T>& a, const EvalPtrs<T>& ep, bool deriv, DBuf<T>& gs, cudaStream_t s) {
   switch (w) {
-    case 6: return launch_eval<T, DIM, 6>(a, ep, gs, s);
-    case 8: return launch_eval<T, DIM, 8>(a, ep, gs, s);
-    case 10: return launch_eval<T, DIM, 10>(a, ep, gs, s);
-    case 12: return launch_eval<T, DIM, 12>(a, ep, gs, s);
-    case 14: return launch_eval<T, DIM, 14>(a, ep, gs, s);
-    default: return launch_eval<T, DIM, 16>(a, ep, gs, s);
+    case 6: return launch_eval<T, DIM, 6>(a, ep, deriv, gs, s);
+    case 8: return launch_eval<T, DIM, 8>(a, ep, deriv, gs, s);
+    case 10: return launch_eval<T, DIM, 10>(a, ep, deriv, gs, s);
+    case 12: return launch_eval<T, DIM, 12>(a, ep, deriv, gs, s);
+    case 14: return launch_eval<T, DIM, 14>(a, ep, deriv, gs, s);
+    default: return launch_eval<T, DIM, 16>(a, ep, deriv, gs, s);
   }
 }
 template <typename T>
-int eval_dim(int dim, int w, PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t s) {
-  if (dim == 1) return eval_w<T, 1>(w, a, ep, gs, s);
-  if (dim == 2) return eval_w<T, 2>(w, a, ep, gs, s);
-  return eval_w<T, 3>(w, a, ep, gs, s);
+int eval_dim(int dim, int w, PWArgs<T>& a, const EvalPtrs<T>& ep, bool deriv, DBuf<T>& gs,
+             cudaStream_t s) {
+  if (dim == 1) return eval_w<T, 1>(w, a, ep, deriv, gs, s);
+  if (dim == 2) return eval_w<T, 2>(w, a, ep, deriv, gs, s);
+  return eval_w<T, 3>(w, a, ep, deriv, gs, s);
 }
 
 void legendre(int nq, std::vector<double>& xq, std::vector<double>& wq) {
@@ -1085,13 +1553,15 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   const bool u0 = e0.pgh > 0 && e0.n > 0, u1 = e1.pgh > 0 && e1.n > 0;
   if (!(u0 || u1) || L.n_eval <= 0) return 0;
   const int pgh_max = std::max(u0 ? e0.pgh : 0, u1 ? e1.pgh : 0);
-  // grid of the evaluation: pot (w), pot+grad through the kernel derivative
-  // (w+2), or one grid per component when hessians are requested (w)
-  // one grid per output component (pot, grad_k, hess_kl), thread-per-point
-  // interpolation in bank-balanced order
-  (void)pgh_max;
-  const int mode = 2;
+  // Grids of the evaluation: potential only (width w); potential and
+  // gradient from one grid through the kernel derivative, whose aliasing
+  // error at width w+2 is below that of the potential at width w; one grid
+  // per output component (pot, grad_k, hess_kl) at width w when hessians are
+  // requested or w+2 exceeds the widest kernel.
+  const bool deriv = pgh_max == 2 && P.w + 2 <= 16;
+  const int mode = deriv ? 1 : 2;
   PWParams Pe = P;
+  if (deriv) pw_grid(Pe, P.w + 2);
   PWArgs<T> a;
   DevTables<T> tb;
   make_args<T>(Pe, a, tb, s, false);
@@ -1131,7 +1601,7 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   if (nbig > 0) {
     ep.boxes = lbig;
     ep.nbox = nbig;
-    launches += eval_dim<T>(P.dim, Pe.w, a, ep, gs, s);
+    launches += eval_dim<T>(P.dim, Pe.w, a, ep, deriv, gs, s);
     if (work) work->n_nufft += nbig;
   }
   int nsmall = L.n_eval - nbig;
@@ -1152,6 +1622,7 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
     FGT_CUDA(cudaStreamSynchronize(s));
     const double wd = pow((double)Pe.w, P.dim);
     const double grids = mode == 2 ? ep.ncomp_max : 1;
+    // derivative mode: value and derivative sums along the last dimension
     const double fl_pt = mode == 1 ? 4.0 * wd : 2.0 * wd * grids;
     work->pts_nufft = (double)h[0];
     work->pts_modal = (double)h[1];
