@@ -75,7 +75,7 @@ _lib = None
 # every symbol declared in include/fgt_b200.h
 EXPORTS = ["fgt_opts_default", "fgt_pfgt_c", "pfgt_", "pfgt_direct_", "fgt_last_status",
            "fgt_last_error", "fgt_version", "fgt_debug_tree_build", "fgt_debug_tree_get",
-           "fgt_debug_tree_free"]
+           "fgt_debug_tree_free", "fgt_direct_nomalloc"]
 
 
 def lib():

@@ -126,6 +126,35 @@ void pfgt_direct_(const int *nd, const int *dim, const double *delta,
                   const double *targ, const int *ifpgh, double *pot,
                   double *grad, double *hess);
 
+/*
+ * Allocation-free variant of the FP64 all-pairs direct sum behind
+ * pfgt_direct_; it has no counterpart in the reference.  For callers that
+ * cannot allocate device memory: it calls no cudaMalloc, cudaFree or other
+ * allocating routine.  All arrays are DEVICE pointers owned by the caller,
+ * in pfgt_direct's layouts (sources(dim,ns), charge(nd,ns), rnormal(dim,ns),
+ * dipstr(nd,ns), targ(dim,nt), pot(nd,nt), grad(nd,dim,nt),
+ * hess(nd,nhess,nt)); the outputs are incremented.  shifts: host array of
+ * dim doubles added to the sources (periodic images), or NULL.  Sources
+ * closer than sqrt(dmax) interact.  Runs asynchronously on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream) and returns FGT_OK or an
+ * FGT_ERR_* code (message in fgt_last_error()).
+ *
+ * Scratch is a static device array of FGT_NOMALLOC_SCRATCH_BYTES that every
+ * GPU loading the library holds until exit: nt*nd*(1 + dim*[ifpgh>=2] +
+ * nhess*[ifpgh>=3]) doubles must fit in it, else FGT_ERR_UNSUPPORTED.  The
+ * first call on each device resolves the array's address with
+ * cudaGetSymbolAddress; make that first call before any stream capture.
+ * All calls share the array (it is cleared at the start of each call):
+ * calls that overlap on the GPU, on any streams, race.
+ */
+#define FGT_NOMALLOC_SCRATCH_BYTES (8u << 20)
+int fgt_direct_nomalloc(int nd, int dim, double delta, double dmax,
+                        const double *shifts, int ns, const double *sources,
+                        int ifcharge, const double *charge, int ifdipole,
+                        const double *rnormal, const double *dipstr, int nt,
+                        const double *targ, int ifpgh, double *pot,
+                        double *grad, double *hess, void *stream);
+
 /* Status of the last pfgt_/pfgt_direct_ call on this host thread. */
 int fgt_last_status(void);
 
