@@ -48,22 +48,30 @@ __global__ void k_gather_vals(const double* __restrict__ v, int n, int nv,
   }
 }
 
-// out[perm[i]] = sorted[i] for pot/grad/hess in the reference's layouts
-// (dreorderi/dreorderiv, src/common/fmmcommon2d.f:29-90).
-__global__ void k_scatter(const double* __restrict__ srt, int n, int nd, int dim, int pgh,
-                          const uint32_t* __restrict__ perm, double* __restrict__ pot,
-                          double* __restrict__ grad, double* __restrict__ hess) {
-  int nh = dim * (dim + 1) / 2;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    size_t o = perm[i];
+// inv[perm[i]] = i
+__global__ void k_invert(const uint32_t* __restrict__ perm, int n, uint32_t* __restrict__ inv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    inv[perm[i]] = (uint32_t)i;
+}
+
+// out[o] = sorted[inv[o]] for pot/grad/hess in the reference's layouts
+// (dreorderi/dreorderiv, src/common/fmmcommon2d.f:29-90).  Gathering by the
+// inverse permutation keeps the output writes coalesced; the random accesses
+// are reads of whole sectors instead of partial-sector writes.
+__global__ void k_gather_out(const double* __restrict__ srt, int n, int nd, int dim, int pgh,
+                             const uint32_t* __restrict__ inv, double* __restrict__ pot,
+                             double* __restrict__ grad, double* __restrict__ hess) {
+  const int nh = dim * (dim + 1) / 2;
+  for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n; o += gridDim.x * blockDim.x) {
+    const size_t i = inv[o];
     for (int id = 0; id < nd; id++) {
-      pot[o * nd + id] = srt[(size_t)id * n + i];
+      pot[(size_t)o * nd + id] = srt[(size_t)id * n + i];
       if (pgh >= 2)
         for (int k = 0; k < dim; k++)
-          grad[(o * dim + k) * nd + id] = srt[((size_t)(1 + k) * nd + id) * n + i];
+          grad[((size_t)o * dim + k) * nd + id] = srt[((size_t)(1 + k) * nd + id) * n + i];
       if (pgh >= 3)
         for (int m = 0; m < nh; m++)
-          hess[(o * nh + m) * nd + id] = srt[((size_t)(1 + dim + m) * nd + id) * n + i];
+          hess[((size_t)o * nh + m) * nd + id] = srt[((size_t)(1 + dim + m) * nd + id) * n + i];
     }
   }
 }
@@ -286,17 +294,24 @@ void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
   launches += direct_near_field<T>(g, L, src, es, &pairs, s);
   tm.mark(7);
   // --- back to input order
-  if (c.ifpgh >= 1) {
-    k_scatter<<<grid_for(c.ns, 256), 256, 0, s>>>(outs, c.ns, nd, dim, c.ifpgh, t.isrc, c.pot,
-                                                  c.grad, c.hess);
-    FGT_LAUNCH_CHECK();
-    launches++;
-  }
-  if (c.ifpghtarg >= 1 && c.nt > 0) {
-    k_scatter<<<grid_for(c.nt, 256), 256, 0, s>>>(outt, c.nt, nd, dim, c.ifpghtarg, t.itrg,
-                                                  c.pott, c.gradt, c.hesst);
-    FGT_LAUNCH_CHECK();
-    launches++;
+  {
+    DBuf<uint32_t> inv(std::max(std::max(c.ns, c.nt), 1), s);
+    if (c.ifpgh >= 1) {
+      k_invert<<<grid_for(c.ns, 256), 256, 0, s>>>(t.isrc, c.ns, inv);
+      FGT_LAUNCH_CHECK();
+      k_gather_out<<<grid_for(c.ns, 256), 256, 0, s>>>(outs, c.ns, nd, dim, c.ifpgh, inv, c.pot,
+                                                       c.grad, c.hess);
+      FGT_LAUNCH_CHECK();
+      launches += 2;
+    }
+    if (c.ifpghtarg >= 1 && c.nt > 0) {
+      k_invert<<<grid_for(c.nt, 256), 256, 0, s>>>(t.itrg, c.nt, inv);
+      FGT_LAUNCH_CHECK();
+      k_gather_out<<<grid_for(c.nt, 256), 256, 0, s>>>(outt, c.nt, nd, dim, c.ifpghtarg, inv,
+                                                       c.pott, c.gradt, c.hesst);
+      FGT_LAUNCH_CHECK();
+      launches += 2;
+    }
   }
   tm.mark(8);
   if (st) {

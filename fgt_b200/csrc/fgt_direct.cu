@@ -208,6 +208,182 @@ __global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
   }
 }
 
+// FP32 variant (mixed precision): each staged source is two float4s,
+// (x_hi, y_hi, z_hi, q) and (x_lo, y_lo, z_lo, dipole strength), read as
+// 128-bit broadcasts, and the cut-off is a select (e = 0 beyond dmax) instead
+// of a divergent branch: the lanes of a warp hold different targets, so a
+// branch would run the pair arithmetic anyway with most lanes idle.
+template <int DIM, int PGH, bool CHG, bool DIP, int NDC>
+__global__ void __launch_bounds__(DW * 32) k_direct32(DArgs<float> a) {
+  constexpr int NH = DIM * (DIM + 1) / 2;
+  constexpr int NC = 1 + (PGH >= 2 ? DIM : 0) + (PGH >= 3 ? NH : 0);
+  constexpr bool PACKQ = NDC == 1;  // charge / dipole strength in the w slots
+  __shared__ float4 shi[DW][32], slo[DW][32];
+  __shared__ float4 snr[DW][DIP ? 32 : 1];
+  __shared__ float sq[DW][CHG && !PACKQ ? NDC : 1][32];
+  __shared__ float sd[DW][DIP && !PACKQ ? NDC : 1][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ndc = min(NDC, a.nd - a.d0);
+  const float ce = a.dinv * 1.4426950408889634f;  // exp(-rr/delta) = 2^(-rr*ce)
+  for (int it = blockIdx.x * DW + warp; it < a.n_items; it += gridDim.x * DW) {
+    const int tb = a.item_box[it];
+    const int p = a.item_lo[it] + lane;
+    const bool act = p < a.e_hi[tb];
+    float tx[3] = {0, 0, 0}, txl[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < DIM; k++) {
+      const double v = act ? a.eoff[(size_t)k * a.ne + p] : 0.0;
+      tx[k] = (float)v;
+      txl[k] = (float)(v - (double)tx[k]);
+    }
+    float acc[NDC][NC];
+    double accd[NDC][NC];
+#pragma unroll
+    for (int i = 0; i < NDC; i++)
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        acc[i][c] = 0.f;
+        accd[i][c] = 0.0;
+      }
+    double cT[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; k++) cT[k] = a.center[(size_t)tb * DIM + k];
+    for (int li = a.l1_ptr[tb]; li < a.l1_ptr[tb + 1]; li++) {
+      const int sb = a.l1_src[li];
+      double dc[DIM];
+#pragma unroll
+      for (int k = 0; k < DIM; k++) {
+        double cs = a.center[(size_t)sb * DIM + k];
+        double sh = 0;
+        if (a.iperiod0 == 1) {  // pfgt_find_local_shift, src/pfgt/pfgt_direct.f:620-651
+          double dx = cT[k] - cs, dxp1 = dx - a.bs0, dxm1 = dx + a.bs0;
+          if (fabs(dx) > fabs(dxp1)) { dx = dxp1; sh = a.bs0; }
+          if (fabs(dx) > fabs(dxm1)) sh = -a.bs0;
+        }
+        dc[k] = (cs + sh) - cT[k];
+      }
+      const int s0 = a.s_lo[sb], s1 = a.s_hi[sb];
+      for (int base = s0; base < s1; base += 32) {
+        const int j = base + lane;
+        __syncwarp();
+        if (j < s1) {
+          float h[3] = {0, 0, 0}, l[3] = {0, 0, 0};
+#pragma unroll
+          for (int k = 0; k < DIM; k++) {
+            const double v = a.soff[(size_t)k * a.ns + j] + dc[k];
+            h[k] = (float)v;
+            l[k] = (float)(v - (double)h[k]);
+          }
+          const float qv = CHG && PACKQ ? a.q[(size_t)a.d0 * a.ns + j] : 0.f;
+          const float dv = DIP && PACKQ ? a.ds[(size_t)a.d0 * a.ns + j] : 0.f;
+          shi[warp][lane] = make_float4(h[0], h[1], h[2], qv);
+          slo[warp][lane] = make_float4(l[0], l[1], l[2], dv);
+          if (DIP) {
+            float r[3] = {0, 0, 0};
+#pragma unroll
+            for (int k = 0; k < DIM; k++) r[k] = a.rn[(size_t)k * a.ns + j];
+            snr[warp][DIP ? lane : 0] = make_float4(r[0], r[1], r[2], 0.f);
+          }
+          if (CHG && !PACKQ)
+#pragma unroll
+            for (int i = 0; i < NDC; i++)
+              if (i < ndc) sq[warp][i][lane] = a.q[(size_t)(a.d0 + i) * a.ns + j];
+          if (DIP && !PACKQ)
+#pragma unroll
+            for (int i = 0; i < NDC; i++)
+              if (i < ndc) sd[warp][i][lane] = a.ds[(size_t)(a.d0 + i) * a.ns + j];
+        }
+        __syncwarp();
+        const int cnt = min(32, s1 - base);
+#pragma unroll 2
+        for (int jj = 0; jj < cnt; jj++) {
+          const float4 hs = shi[warp][jj], ls = slo[warp][jj];
+          const float hv[3] = {hs.x, hs.y, hs.z}, lv[3] = {ls.x, ls.y, ls.z};
+          float dr[DIM], rr = 0.f;
+#pragma unroll
+          for (int k = 0; k < DIM; k++) {
+            dr[k] = (tx[k] - hv[k]) + (txl[k] - lv[k]);
+            rr = fmaf(dr[k], dr[k], rr);
+          }
+          const float e = rr < a.dmax ? fgt_ex2(-rr * ce) : 0.f;
+          if (CHG) {
+            // gnd_directc{p,g,h}, src/pfgt/pfgt_direct.f:47-196
+            float dg[DIM];
+#pragma unroll
+            for (int k = 0; k < DIM; k++) dg[k] = -a.rfac * dr[k];
+#pragma unroll
+            for (int i = 0; i < NDC; i++) {
+              if (i >= ndc) break;
+              const float r = e * (PACKQ ? hs.w : sq[warp][i][jj]);
+              acc[i][0] += r;
+              if (PGH >= 2)
+#pragma unroll
+                for (int k = 0; k < DIM; k++) acc[i][1 + k] = fmaf(dg[k], r, acc[i][1 + k]);
+              if (PGH >= 3)
+#pragma unroll
+                for (int m = 0; m < NH; m++) {
+                  const int ka = HessIdx<DIM>::a(m), kb = HessIdx<DIM>::b(m);
+                  const float hh = dg[ka] * dg[kb] + (ka == kb ? -a.rfac : 0.f);
+                  acc[i][1 + DIM + m] = fmaf(hh, r, acc[i][1 + DIM + m]);
+                }
+            }
+          }
+          if (DIP) {
+            // gnd_directd{p,g,h}, src/pfgt/pfgt_direct.f:204-384
+            const float4 ns4 = snr[warp][DIP ? jj : 0];
+            const float nv[3] = {ns4.x, ns4.y, ns4.z};
+            float d[DIM], rn[DIM], rinc = 0.f;
+#pragma unroll
+            for (int k = 0; k < DIM; k++) {
+              d[k] = a.rfac * dr[k];
+              rn[k] = nv[k];
+              rinc = fmaf(d[k], rn[k], rinc);
+            }
+            float rg[DIM];
+#pragma unroll
+            for (int k = 0; k < DIM; k++) rg[k] = rn[k] * a.rfac - rinc * d[k];
+#pragma unroll
+            for (int i = 0; i < NDC; i++) {
+              if (i >= ndc) break;
+              const float r = e * (PACKQ ? ls.w : sd[warp][i][jj]);
+              acc[i][0] = fmaf(rinc, r, acc[i][0]);
+              if (PGH >= 2)
+#pragma unroll
+                for (int k = 0; k < DIM; k++) acc[i][1 + k] = fmaf(rg[k], r, acc[i][1 + k]);
+              if (PGH >= 3)
+#pragma unroll
+                for (int m = 0; m < NH; m++) {
+                  const int ka = HessIdx<DIM>::a(m), kb = HessIdx<DIM>::b(m);
+                  const float hh = (ka == kb) ? (-a.rfac * (d[ka] * rn[ka] + rinc) - rg[ka] * d[ka])
+                                              : (-a.rfac * d[ka] * rn[kb] - rg[ka] * d[kb]);
+                  acc[i][1 + DIM + m] = fmaf(hh, r, acc[i][1 + DIM + m]);
+                }
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < NDC; i++)
+#pragma unroll
+          for (int c = 0; c < NC; c++) {
+            accd[i][c] += (double)acc[i][c];
+            acc[i][c] = 0.f;
+          }
+      }
+    }
+    if (act) {
+#pragma unroll
+      for (int i = 0; i < NDC; i++) {
+        if (i >= ndc) break;
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          double* o = &a.out[((size_t)c * a.nd + a.d0 + i) * a.ne + p];
+          *o += accd[i][c] + (double)acc[i][c];
+        }
+      }
+    }
+  }
+}
+
 __global__ void k_items_count(int nboxes, const int* __restrict__ l1_ptr, const int* __restrict__ lo,
                               const int* __restrict__ hi, const int* __restrict__ s_lo,
                               const int* __restrict__ s_hi, const int* __restrict__ l1_src,
@@ -235,7 +411,10 @@ __global__ void k_items_fill(int nboxes, const int* __restrict__ cnt, const int*
 template <typename T, int DIM, int PGH, bool CHG, bool DIP, int NDC>
 void launch_direct(const DArgs<T>& a, cudaStream_t s) {
   int grid = std::max(1, std::min(ceil_div(a.n_items, DW), kSMs * 16));
-  k_direct<T, DIM, PGH, CHG, DIP, NDC><<<grid, DW * 32, 0, s>>>(a);
+  if constexpr (sizeof(T) == 4)
+    k_direct32<DIM, PGH, CHG, DIP, NDC><<<grid, DW * 32, 0, s>>>(a);
+  else
+    k_direct<T, DIM, PGH, CHG, DIP, NDC><<<grid, DW * 32, 0, s>>>(a);
   FGT_LAUNCH_CHECK();
 }
 

@@ -1,0 +1,626 @@
+// Device helpers shared by the plane-wave form/translate kernels (K6, K7,
+// fgt_pw.cu) and the evaluation kernels (K8, fgt_pw_eval.cu).
+//
+// Per box, one CTA keeps the whole spreading sub-grid in shared memory (a
+// global-memory slice per CTA when it does not fit): spread (ES kernel,
+// Barnett-Magland-af Klinteberg 2019) -> in-place pruned DFT passes along the
+// last, middle and first dimension -> deconvolution and PW weights fused into
+// the pass that writes the expansion.  Only the sub-grid the box's points can
+// reach is stored: for boxes of the cut-off size the scaled coordinates lie
+// in [-pi/3, pi/3], about a third of the 2*pi period.
+//
+// 3D FP32 spreading accumulates blocks of points in register tiles
+// (spread_tiled); the other spreading variants and the interpolation are
+// thread-per-point over a bank-balanced processing order of each box's
+// points (see order_chunk), so the 32 lanes of a warp touch 32 distinct
+// shared-memory banks at every stencil offset.
+#pragma once
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "fgt_pw.cuh"
+
+namespace fgt {
+
+namespace {
+
+constexpr int PW_THREADS = 512;
+constexpr int MODAL_THREADS = 256;
+constexpr int ORDER_CHUNK = 2048;  // points ordered per round (u16 indices)
+constexpr int MAXSMEM = 227 * 1024;
+
+struct Geo {
+  int dim, K, G, l0, nf, wrap, nexp, nd;
+  int S[3], str[3];  // buffer extents and strides (T units) per dim
+  int bufsz;
+};
+
+template <typename T>
+struct PWArgs {
+  Geo g;
+  T halfw_over_dx, inv_hw, beta, dscale;  // inv_hw = dx / halfw
+  double scale_d, inv_dx_d, hwdx_d;  // FP64 positions (points are FP64 offsets)
+  const T* twf;   // [G][2K+1] fwd full
+  const T* twh;   // [G][K+1]  fwd half
+  const T* tif;   // [2K+1][G] inv full
+  const T* tih;   // [K+1][G]  inv half (with 1/2/2/.. weights)
+  const T* facf;  // [2K+1] dx*wsym/phihat
+  const T* faci;  // [2K+1] dx/phihat
+  const T* ts;    // [2K+1] ts(k)
+  T inv_sqd0;
+  T* gscratch;  // global buffer slices when the grid does not fit in smem
+};
+
+// byte offset of the grid buffer in shared memory: twiddles, then the
+// ordering scratch (ORDER_CHUNK ints + 32 counters + ORDER_CHUNK u16)
+template <typename T>
+__host__ __device__ constexpr size_t order_offset(int G, int K) {
+  return (((size_t)sizeof(T) * 2 * G * ((2 * K + 1) + (K + 1)) +
+           sizeof(int) * (ORDER_CHUNK + 32) + sizeof(unsigned short) * ORDER_CHUNK) + 15) &
+         ~(size_t)15;
+}
+
+// ---------------------------------------------------------------- passes
+// In-place line transforms over whole lines per round (a line is read
+// completely before any of its outputs is written).
+// MODE 0: real -> half complex (fwd, last dim), MODE 1: complex -> complex,
+// MODE 2: half complex -> real (inv, last dim).
+template <typename T, int MODE>
+__device__ __forceinline__ void pass_inplace(T* B, int nl, int nb, int SA, int SB, int ein,
+                                             int eout, int nin, int nout, const T* __restrict__ tw) {
+  // register tile: LG lines x KG outputs per thread; a round covers whole
+  // lines (all of a line's inputs are read before any output is written)
+  constexpr int LG = 2, KG = sizeof(T) == 4 ? 4 : 2;
+  const int nkg = (nout + KG - 1) / KG;
+  const int ngroups = blockDim.x / nkg;
+  const int t = threadIdx.x, lg = t / nkg, kg = t - lg * nkg;
+  const bool act_t = lg < ngroups;
+  const int lpr = ngroups * LG;
+  for (int r0 = 0; r0 < nl; r0 += lpr) {
+    T re[LG][KG], im[LG][KG];
+    int base[LG];
+    bool lact[LG];
+#pragma unroll
+    for (int g = 0; g < LG; g++) {
+      const int line = r0 + lg * LG + g;
+      lact[g] = act_t && line < nl;
+      base[g] = lact[g] ? (line / nb) * SA + (line % nb) * SB : 0;
+#pragma unroll
+      for (int j = 0; j < KG; j++) re[g][j] = im[g][j] = T(0);
+    }
+    if (act_t) {
+      for (int l = 0; l < nin; l++) {
+        T tr[KG], ti[KG];
+#pragma unroll
+        for (int j = 0; j < KG; j++) {
+          const int k = kg * KG + j;
+          const bool ok = k < nout;
+          tr[j] = ok ? tw[2 * (l * nout + k)] : T(0);
+          ti[j] = ok ? tw[2 * (l * nout + k) + 1] : T(0);
+        }
+#pragma unroll
+        for (int g = 0; g < LG; g++) {
+          if (!lact[g]) continue;
+          if (MODE == 0) {
+            const T gv = B[base[g] + l * ein];
+#pragma unroll
+            for (int j = 0; j < KG; j++) {
+              re[g][j] += gv * tr[j];
+              im[g][j] += gv * ti[j];
+            }
+          } else {
+            const T xr = B[base[g] + l * ein], xi = B[base[g] + l * ein + 1];
+#pragma unroll
+            for (int j = 0; j < KG; j++) {
+              re[g][j] += xr * tr[j] - xi * ti[j];
+              if (MODE == 1) im[g][j] += xr * ti[j] + xi * tr[j];
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int g = 0; g < LG; g++) {
+      if (!lact[g]) continue;
+#pragma unroll
+      for (int j = 0; j < KG; j++) {
+        const int k = kg * KG + j;
+        if (k >= nout) break;
+        if (MODE == 2) {
+          B[base[g] + k * eout] = re[g][j];
+        } else {
+          B[base[g] + k * eout] = re[g][j];
+          B[base[g] + k * eout + 1] = im[g][j];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ES kernel exp(beta (sqrt(1 - z^2) - 1)) with the exponent written as
+// -beta z^2 / (1 + sqrt(1 - z^2)): no cancellation near the peak, where the
+// direct form loses beta * 2^-24 of relative accuracy in FP32.
+template <typename T>
+__device__ __forceinline__ T es_kernel(T z, T beta) {
+  const T q = T(1) - z * z;
+  const T r = q > T(0) ? q * Real<T>::rsqrt_(q) : T(0);
+  return Real<T>::expm(Real<T>::div12(beta * (z * z), T(1) + r));
+}
+
+__device__ __forceinline__ int pmod(int a, int n) {
+  int c = a % n;
+  return c < 0 ? c + n : c;
+}
+
+// Stencil cell offsets (T units) along each dimension.  Lin: the sub-grid
+// case, cells base..base+W-1 (offsets fold into address immediates); Tab:
+// the periodic full grid, cells wrap modulo nf (one modulo per dimension).
+// ki[i] for a run-time i without demoting ki to local memory
+__device__ __forceinline__ int sel3(const int* ki, int i) {
+  return i == 0 ? ki[0] : (i == 1 ? ki[1] : ki[2]);
+}
+
+template <int DIM, int W>
+struct LinIdx {
+  int o[DIM];
+  int str0, str1;
+  __device__ __forceinline__ LinIdx(const Geo& g, const int* s) : str0(g.str[0]), str1(g.str[1]) {
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      int b = s[d] - g.l0;
+      b = b < 0 ? 0 : (b > g.G - W ? g.G - W : b);
+      o[d] = b * g.str[d];
+    }
+  }
+  __device__ __forceinline__ int x(int j) const { return o[0] + j * (DIM == 1 ? 1 : str0); }
+  __device__ __forceinline__ int y(int j) const { return o[1] + j * (DIM == 2 ? 1 : str1); }
+  __device__ __forceinline__ int z(int j) const { return o[DIM - 1] + j; }
+};
+template <int DIM, int W>
+struct TabIdx {
+  int o[DIM][W];
+  __device__ __forceinline__ TabIdx(const Geo& g, const int* s) {
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      int c = pmod(s[d], g.nf);
+#pragma unroll
+      for (int j = 0; j < W; j++) {
+        o[d][j] = c * g.str[d];
+        c = c + 1 == g.nf ? 0 : c + 1;
+      }
+    }
+  }
+  __device__ __forceinline__ int x(int j) const { return o[0][j]; }
+  __device__ __forceinline__ int y(int j) const { return o[1][j]; }
+  __device__ __forceinline__ int z(int j) const { return o[DIM - 1][j]; }
+};
+
+// Calls body(x offset, weight) for the W cells of a stencil's outer dimension
+// with every register-array index a compile-time constant, so the kernel
+// values never go to local memory: fully unrolled for W <= U, otherwise a
+// rolled loop over rotating registers.
+template <typename T, int W, int U, class IX, class F>
+__device__ __forceinline__ void outer_cells(const IX& ix, const T* ph0, F&& body) {
+  if constexpr (W <= U) {
+#pragma unroll
+    for (int j = 0; j < W; j++) body(ix.x(j), ph0[j]);
+  } else {
+    int xo[W];
+    T pw[W];
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+      xo[j] = ix.x(j);
+      pw[j] = ph0[j];
+    }
+#pragma unroll 1
+    for (int j = 0; j < W; j++) {
+      body(xo[0], pw[0]);
+#pragma unroll
+      for (int k = 0; k + 1 < W; k++) {
+        xo[k] = xo[k + 1];
+        pw[k] = pw[k + 1];
+      }
+    }
+  }
+}
+
+template <typename T, int DIM, int W, class IX>
+__device__ __forceinline__ T interp_cells(const T* B, const IX& ix, const T (*ph)[W]) {
+  T acc = T(0);
+  if constexpr (DIM == 1) {
+#pragma unroll
+    for (int j = 0; j < W; j++) acc += B[ix.x(j)] * ph[0][j];
+  } else if constexpr (DIM == 2) {
+    outer_cells<T, W, 16>(ix, ph[0], [&](int xo, T p0) {
+      const T* bx = B + xo;
+      T sy = T(0);
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) sy += bx[ix.z(jy)] * ph[1][jy];
+      acc += sy * p0;
+    });
+  } else {
+    outer_cells<T, W, 8>(ix, ph[0], [&](int xo, T p0) {
+      const T* bx = B + xo;
+      T sx = T(0);
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        const T* bxy = bx + ix.y(jy);
+        T sy = T(0);
+#pragma unroll
+        for (int jz = 0; jz < W; jz++) sy += bxy[ix.z(jz)] * ph[2][jz];
+        sx += sy * ph[1][jy];
+      }
+      acc += sx * p0;
+    });
+  }
+  return acc;
+}
+
+template <typename T, int DIM, int W, class IX>
+__device__ __forceinline__ void spread_cells(T* B, const IX& ix, const T (*ph)[W], T str) {
+  if constexpr (DIM == 1) {
+#pragma unroll
+    for (int j = 0; j < W; j++) atomicAdd(B + ix.x(j), str * ph[0][j]);
+  } else if constexpr (DIM == 2) {
+    outer_cells<T, W, 16>(ix, ph[0], [&](int xo, T p0) {
+      T* bx = B + xo;
+      const T v = str * p0;
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) atomicAdd(bx + ix.z(jy), v * ph[1][jy]);
+    });
+  } else {
+    outer_cells<T, W, 8>(ix, ph[0], [&](int xo, T p0) {
+      T* bx = B + xo;
+      const T vx = str * p0;
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        T* bxy = bx + ix.y(jy);
+        const T vxy = vx * ph[1][jy];
+#pragma unroll
+        for (int jz = 0; jz < W; jz++) atomicAdd(bxy + ix.z(jz), vxy * ph[2][jz]);
+      }
+    });
+  }
+}
+
+// Thread-per-point interpolation (component grids of the hessian path).
+template <typename T, int W>
+__device__ __forceinline__ int kernel_row(const PWArgs<T>& a, double x, T* phi) {
+  const double u = x * a.inv_dx_d;
+  const int i0 = (int)ceil(u - a.hwdx_d);
+  const T f0 = (T)((double)i0 - u);
+#pragma unroll
+  for (int j = 0; j < W; j++) phi[j] = es_kernel<T>((f0 + (T)j) * a.inv_hw, a.beta);
+  return i0;
+}
+
+template <typename T, int DIM, int W>
+__device__ __forceinline__ T interp_point(const PWArgs<T>& a, const T* B, const double* x) {
+  T ph[DIM][W];
+  int s[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) s[d] = kernel_row<T, W>(a, x[d], ph[d]);
+  if (a.g.wrap) return interp_cells<T, DIM, W>(B, TabIdx<DIM, W>(a.g, s), ph);
+  return interp_cells<T, DIM, W>(B, LinIdx<DIM, W>(a.g, s), ph);
+}
+
+template <typename T, int DIM, int W>
+__device__ __forceinline__ void spread_point(const PWArgs<T>& a, T* B, const double* x, T str) {
+  T ph[DIM][W];
+  int s[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) s[d] = kernel_row<T, W>(a, x[d], ph[d]);
+  if (a.g.wrap)
+    spread_cells<T, DIM, W>(B, TabIdx<DIM, W>(a.g, s), ph, str);
+  else
+    spread_cells<T, DIM, W>(B, LinIdx<DIM, W>(a.g, s), ph, str);
+}
+
+// Kernel values and their derivatives with respect to the point's original
+// coordinate: d/dx phi((x_c - x)/halfw) = phi * beta * z / (sqrt(1-z^2) halfw),
+// times the coordinate scale (a.dscale = scale / halfw).  Zero at |z| = 1.
+template <typename T, int W>
+__device__ __forceinline__ int kernel_row_d(const PWArgs<T>& a, double x, T* phi, T* dphi) {
+  const double u = x * a.inv_dx_d;
+  const int i0 = (int)ceil(u - a.hwdx_d);
+  const T f0 = (T)((double)i0 - u);
+#pragma unroll
+  for (int j = 0; j < W; j++) {
+    const T z = (f0 + (T)j) * a.inv_hw;
+    const T q = T(1) - z * z;
+    const T rq = q > T(0) ? Real<T>::rsqrt_(q) : T(0);
+    const T e = Real<T>::expm(Real<T>::div12(a.beta * (z * z), T(1) + q * rq));
+    phi[j] = e;
+    dphi[j] = e * (a.beta * a.dscale) * z * rq;
+  }
+  return i0;
+}
+
+// outer_cells with a second weight row (value and derivative along x)
+template <typename T, int W, int U, class IX, class F>
+__device__ __forceinline__ void outer_cells2(const IX& ix, const T* p0, const T* q0, F&& body) {
+  if constexpr (W <= U) {
+#pragma unroll
+    for (int j = 0; j < W; j++) body(ix.x(j), p0[j], q0[j]);
+  } else {
+    int xo[W];
+    T pw[W], qw[W];
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+      xo[j] = ix.x(j);
+      pw[j] = p0[j];
+      qw[j] = q0[j];
+    }
+#pragma unroll 1
+    for (int j = 0; j < W; j++) {
+      body(xo[0], pw[0], qw[0]);
+#pragma unroll
+      for (int k = 0; k + 1 < W; k++) {
+        xo[k] = xo[k + 1];
+        pw[k] = pw[k + 1];
+        qw[k] = qw[k + 1];
+      }
+    }
+  }
+}
+
+// Potential and gradient of one grid at one point: v[0] = pot, v[1+d] = d/dx_d.
+// The sums run over B - Bref (Bref = the stencil's centre cell): the
+// derivative stencils sum to the derivative of the kernel's partition of
+// unity, which is at the aliasing level, so dropping Bref from them changes
+// nothing, while the smaller summands keep the FP32 sums from cancelling
+// when the field varies slowly over the stencil.  The potential adds Bref
+// times the product of the kernel row sums back.
+template <typename T, int DIM, int W, class IX>
+__device__ __forceinline__ void interp_grad_cells(const T* B, const IX& ix, const T (*ph)[W],
+                                                  const T (*dph)[W], T* v) {
+  T ksum = T(1);
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    T sd = T(0);
+#pragma unroll
+    for (int j = 0; j < W; j++) sd += ph[d][j];
+    ksum *= sd;
+  }
+  if constexpr (DIM == 1) {
+    const T bref = B[ix.x(W / 2)];
+    T s0 = T(0), s1 = T(0);
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+      const T b = B[ix.x(j)] - bref;
+      s0 += b * ph[0][j];
+      s1 += b * dph[0][j];
+    }
+    v[0] = s0 + bref * ksum;
+    v[1] = s1;
+  } else if constexpr (DIM == 2) {
+    const T bref = B[ix.x(W / 2) + ix.z(W / 2)];
+    T pot = T(0), gx = T(0), gy = T(0);
+    outer_cells2<T, W, 16>(ix, ph[0], dph[0], [&](int xo, T px, T dpx) {
+      const T* bx = B + xo;
+      T s0 = T(0), s1 = T(0);
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        const T b = bx[ix.z(jy)] - bref;
+        s0 += b * ph[1][jy];
+        s1 += b * dph[1][jy];
+      }
+      pot += px * s0;
+      gx += dpx * s0;
+      gy += px * s1;
+    });
+    v[0] = pot + bref * ksum;
+    v[1] = gx;
+    v[2] = gy;
+  } else {
+    const T bref = B[ix.x(W / 2) + ix.y(W / 2) + ix.z(W / 2)];
+    T pot = T(0), gx = T(0), gy = T(0), gz = T(0);
+    outer_cells2<T, W, 8>(ix, ph[0], dph[0], [&](int xo, T px, T dpx) {
+      const T* bx = B + xo;
+      T t0 = T(0), t1 = T(0), t2 = T(0);
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        const T* bxy = bx + ix.y(jy);
+        T s0 = T(0), s1 = T(0);
+#pragma unroll
+        for (int jz = 0; jz < W; jz++) {
+          const T b = bxy[ix.z(jz)] - bref;
+          s0 += b * ph[2][jz];
+          s1 += b * dph[2][jz];
+        }
+        t0 += ph[1][jy] * s0;
+        t1 += dph[1][jy] * s0;
+        t2 += ph[1][jy] * s1;
+      }
+      pot += px * t0;
+      gx += dpx * t0;
+      gy += px * t1;
+      gz += px * t2;
+    });
+    v[0] = pot + bref * ksum;
+    v[1] = gx;
+    v[2] = gy;
+    v[3] = gz;
+  }
+}
+
+template <typename T, int DIM, int W>
+__device__ __forceinline__ void interp_grad_point(const PWArgs<T>& a, const T* B, const double* x,
+                                                  T* v) {
+  T ph[DIM][W], dph[DIM][W];
+  int s[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) s[d] = kernel_row_d<T, W>(a, x[d], ph[d], dph[d]);
+  if (a.g.wrap)
+    interp_grad_cells<T, DIM, W>(B, TabIdx<DIM, W>(a.g, s), ph, dph, v);
+  else
+    interp_grad_cells<T, DIM, W>(B, LinIdx<DIM, W>(a.g, s), ph, dph, v);
+}
+
+// Bank-balanced processing order of a chunk of points.  Thread-per-point
+// stencils touch B[base_p + offset] for the same offset in every lane at
+// once; ordering the chunk by (rank within bank class, bank class) with
+// class = base_p mod NCLASS puts NCLASS different classes into every run of
+// NCLASS consecutive points, so those accesses hit distinct banks.
+template <typename T, int DIM, int W>
+__device__ __forceinline__ void order_chunk(const PWArgs<T>& a, const double* off, int ne, int q0,
+                                            int n, unsigned short* perm, int* tmp, int* cnt) {
+  constexpr int NCLASS = sizeof(T) == 4 ? 32 : 16;  // 4-byte banks
+  const Geo& g = a.g;
+  if (threadIdx.x < NCLASS) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int base = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const double u = off[(size_t)d * ne + q0 + i] * a.scale_d * a.inv_dx_d;
+      const int i0 = (int)ceil(u - a.hwdx_d);
+      int b = g.wrap ? pmod(i0, g.nf) : i0 - g.l0;
+      if (!g.wrap) b = b < 0 ? 0 : (b > g.G - W ? g.G - W : b);
+      base += b * g.str[d];
+    }
+    const int cls = base & (NCLASS - 1);
+    const int rank = atomicAdd(&cnt[cls], 1);
+    tmp[i] = rank * NCLASS + cls;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int rank = tmp[i] / NCLASS, cls = tmp[i] % NCLASS;
+    int pos = 0;
+#pragma unroll 8
+    for (int c = 0; c < NCLASS; c++) {
+      const int k = cnt[c];
+      pos += k < rank ? k : rank;
+      pos += (c < cls && k > rank) ? 1 : 0;
+    }
+    perm[pos] = (unsigned short)i;
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ __forceinline__ void load_tw(T* dst, const T* src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+int supported_w(int w) {
+  const int ws[] = {6, 8, 10, 12, 14, 16};
+  for (int v : ws)
+    if (w <= v) return v;
+  return 16;
+}
+
+template <typename T>
+struct DevTables {
+  DBuf<T> twf, twh, tif, tih, facf, faci, ts;
+};
+
+// Device arguments for grid parameters P; the innermost buffer stride is
+// padded to W (mod 32) words for FP32 so the warp-per-point stencils are
+// bank-conflict free.
+template <typename T>
+void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s, bool pad) {
+  Geo& g = a.g;
+  g.dim = P.dim;
+  g.K = P.K;
+  g.G = P.G;
+  g.l0 = P.l0;
+  g.nf = P.nf;
+  g.wrap = P.wrap ? 1 : 0;
+  g.nexp = P.nexp;
+  g.nd = P.nd;
+  const int K = P.K, NF = 2 * K + 1, NH = K + 1, G = P.G;
+  int S[3] = {1, 1, 1};
+  if (P.dim == 3) {
+    S[0] = std::max(G, NF);
+    S[1] = std::max(G, NF);
+    S[2] = std::max(G, 2 * NH);
+  } else if (P.dim == 2) {
+    S[0] = std::max(G, NF);
+    S[1] = std::max(G, 2 * NH);
+  } else {
+    S[0] = std::max(G, 2 * NH);
+  }
+  if (pad && sizeof(T) == 4 && P.dim >= 2) {
+    int& last = S[P.dim - 1];
+    while ((last - P.w) % 32 != 0 || (last & 1)) last++;
+  }
+  g.bufsz = 1;
+  for (int d = 0; d < P.dim; d++) g.bufsz *= S[d];
+  for (int d = 0; d < 3; d++) g.S[d] = S[d];
+  g.str[P.dim - 1] = 1;
+  for (int d = P.dim - 2; d >= 0; d--) g.str[d] = g.str[d + 1] * S[d + 1];
+  a.scale_d = P.hpw / P.sqd0;
+  a.inv_dx_d = 1.0 / P.dx;
+  a.hwdx_d = P.halfw / P.dx;
+  a.halfw_over_dx = (T)(P.halfw / P.dx);
+  a.inv_hw = (T)(P.dx / P.halfw);
+  a.beta = (T)P.beta;
+  a.dscale = (T)(a.inv_dx_d * a.scale_d / a.hwdx_d);
+  a.inv_sqd0 = (T)(1.0 / P.sqd0);
+  std::vector<T> twf(2 * G * NF), twh(2 * G * NH), tif(2 * NF * G), tih(2 * NH * G);
+  for (int l = 0; l < G; l++) {
+    double xl = (double)(P.l0 + l) * P.dx;
+    for (int k = -K; k <= K; k++) {
+      double c = cos(k * xl), sn = sin(k * xl);
+      twf[2 * (l * NF + k + K)] = (T)c;
+      twf[2 * (l * NF + k + K) + 1] = (T)(-sn);
+      tif[2 * ((k + K) * G + l)] = (T)c;
+      tif[2 * ((k + K) * G + l) + 1] = (T)sn;
+      if (k >= 0) {
+        twh[2 * (l * NH + k)] = (T)c;
+        twh[2 * (l * NH + k) + 1] = (T)(-sn);
+        double f = k == 0 ? 1.0 : 2.0;
+        tih[2 * (k * G + l)] = (T)(f * c);
+        tih[2 * (k * G + l) + 1] = (T)(f * sn);
+      }
+    }
+  }
+  std::vector<T> facf(NF), faci(NF), ts(NF);
+  for (int k = 0; k < NF; k++) {
+    facf[k] = (T)(P.dx * P.wsym[k] / P.phihat[k]);
+    faci[k] = (T)(P.dx / P.phihat[k]);
+    ts[k] = (T)P.ts[k];
+  }
+  auto up = [&](DBuf<T>& b, const std::vector<T>& h) {
+    b.alloc(h.size(), s);
+    FGT_CUDA(cudaMemcpyAsync(b.get(), h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
+  };
+  up(tb.twf, twf);
+  up(tb.twh, twh);
+  up(tb.tif, tif);
+  up(tb.tih, tih);
+  up(tb.facf, facf);
+  up(tb.faci, faci);
+  up(tb.ts, ts);
+  FGT_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
+  a.twf = tb.twf;
+  a.twh = tb.twh;
+  a.tif = tb.tif;
+  a.tih = tb.tih;
+  a.facf = tb.facf;
+  a.faci = tb.faci;
+  a.ts = tb.ts;
+  a.gscratch = nullptr;
+}
+
+template <typename T>
+size_t fixed_smem(const PWArgs<T>& a, int, int) {
+  return order_offset<T>(a.g.G, a.g.K);
+}
+
+template <typename KernelT>
+void set_smem(KernelT k, size_t bytes) {
+  FGT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+}  // namespace
+
+// flops of the in-place passes of one grid (used for the work counters)
+double pw_pass_flops(const PWParams& P);
+
+}  // namespace fgt

@@ -1,0 +1,512 @@
+// Plane-wave evaluation kernels (K8): per-box grids with interpolation at
+// the box's points, and direct modal sums for boxes with few points.
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "fgt_pw_dev.cuh"
+
+namespace fgt {
+
+namespace {
+
+// ---------------------------------------------------------------- eval
+template <typename T>
+struct EvalPtrs {
+  const T* loc;      // [n_eval][nd][nexp]
+  const int* boxes;  // eval slots handled by this launch
+  const int* eval_box;
+  int nbox;
+  // two evaluation sets (sources, targets)
+  const double* off[2];
+  const int* lo[2];
+  const int* hi[2];
+  double* out[2];
+  int n[2], ncomp[2];
+  int nd, ncomp_max;
+};
+
+// component factor (complex) of evaluation component c at mode ki[]
+template <typename T, int DIM>
+__device__ __forceinline__ void eval_factor(const PWArgs<T>& a, int c, const int* ki, T& fr, T& fi) {
+  if (c == 0) {
+    fr = T(1);
+    fi = T(0);
+    return;
+  }
+  if (c <= DIM) {  // i ts(k_d)/sqrt(delta0)
+    fr = T(0);
+    fi = a.ts[sel3(ki, c - 1)] * a.inv_sqd0;
+    return;
+  }
+  int m = c - 1 - DIM, p, q;
+  if (DIM == 1) { p = 0; q = 0; }
+  else if (DIM == 2) { p = (m == 2) ? 1 : 0; q = (m == 0) ? 0 : 1; }
+  else { p = m < 3 ? m : (m < 5 ? 0 : 1); q = m < 3 ? m : (m == 3 ? 1 : 2); }
+  fr = -a.ts[sel3(ki, p)] * a.ts[sel3(ki, q)] * a.inv_sqd0 * a.inv_sqd0;
+  fi = T(0);
+}
+
+// Grid of evaluation component c of expansion L in buffer B (real values).
+template <typename T, int DIM>
+__device__ __forceinline__ void build_eval_grid(const PWArgs<T>& a, const T* L, int c, T* B,
+                                                const T* tif, const T* tih) {
+  const Geo& g = a.g;
+  const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
+  const int nline = DIM == 3 ? NF * NH : (DIM == 2 ? NH : 1);
+  if (DIM == 1) {
+    for (int l = threadIdx.x; l < G; l += blockDim.x) {
+      T acc = T(0);
+      for (int k = 0; k < NH; k++) {
+        int ki[3] = {k + K, 0, 0};
+        T fr, fi;
+        eval_factor<T, DIM>(a, c, ki, fr, fi);
+        const T f = a.faci[k + K];
+        const T lr = L[2 * k] * f, li = L[2 * k + 1] * f;
+        const T mr = lr * fr - li * fi, mi = lr * fi + li * fr;
+        acc += mr * tih[2 * (k * G + l)] - mi * tih[2 * (k * G + l) + 1];
+      }
+      B[l] = acc;
+    }
+    __syncthreads();
+    return;
+  }
+  // expansion times factors at B[kx][ky][kz], then the x pass in place
+  for (int m = threadIdx.x; m < g.nexp; m += blockDim.x) {
+    int ki[3], pos;
+    if (DIM == 3) {
+      const int kxi = m / nline, line = m - kxi * nline;
+      const int kyi = line / NH, kz = line - kyi * NH;
+      ki[0] = kxi;
+      ki[1] = kyi;
+      ki[2] = kz + K;
+      pos = kxi * g.str[0] + kyi * g.str[1] + 2 * kz;
+    } else {
+      const int kxi = m / NH, ky = m - kxi * NH;
+      ki[0] = kxi;
+      ki[1] = ky + K;
+      pos = kxi * g.str[0] + 2 * ky;
+    }
+    T f = T(1);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) f *= a.faci[ki[d]];
+    T fr, fi;
+    eval_factor<T, DIM>(a, c, ki, fr, fi);
+    fr *= f;
+    fi *= f;
+    const T lr = L[2 * m], li = L[2 * m + 1];
+    B[pos] = lr * fr - li * fi;
+    B[pos + 1] = lr * fi + li * fr;
+  }
+  __syncthreads();
+  if (DIM == 3) {
+    pass_inplace<T, 1>(B, NF * NH, NH, g.str[1], 2, g.str[0], g.str[0], NF, G, tif);
+    pass_inplace<T, 1>(B, G * NH, NH, g.str[0], 2, g.str[1], g.str[1], NF, G, tif);
+    pass_inplace<T, 2>(B, G * G, G, g.str[0], g.str[1], 2, 1, NH, G, tih);
+  } else {
+    pass_inplace<T, 1>(B, NH, 1, 2, 0, g.str[0], g.str[0], NF, G, tif);
+    pass_inplace<T, 2>(B, G, 1, g.str[0], 0, 2, 1, NH, G, tih);
+  }
+}
+
+// Thread-per-point interpolation of both evaluation sets in bank-balanced
+// order.  DERIV: one potential grid, gradients through the kernel derivative
+// (no hessians); otherwise one grid per output component (pot, grad_k,
+// hess_kl).
+template <typename T, int DIM, int W, bool GB, bool DERIV>
+__global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<T> p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Geo& g = a.g;
+  const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  T* tif = sm;
+  T* tih = tif + 2 * NF * G;
+  int* ordtmp = reinterpret_cast<int*>(tih + 2 * NH * G);
+  int* ordcnt = ordtmp + ORDER_CHUNK;
+  unsigned short* perm = reinterpret_cast<unsigned short*>(ordcnt + 32);
+  T* B = GB ? a.gscratch + (size_t)blockIdx.x * g.bufsz
+            : reinterpret_cast<T*>(smem_raw + order_offset<T>(G, K));
+  load_tw(tif, a.tif, 2 * NF * G);
+  load_tw(tih, a.tih, 2 * NH * G);
+  __syncthreads();
+  for (int bi = blockIdx.x; bi < p.nbox; bi += gridDim.x) {
+    const int e = p.boxes[bi];
+    const int box = p.eval_box[e];
+    for (int id = 0; id < p.nd; id++) {
+      const T* L = p.loc + ((size_t)e * p.nd + id) * 2 * g.nexp;
+      for (int c = 0; c < (DERIV ? 1 : p.ncomp_max); c++) {
+        build_eval_grid<T, DIM>(a, L, c, B, tif, tih);
+        for (int set = 0; set < 2; set++) {
+          // select by value: indexing the parameter arrays with a run-time
+          // index would copy them to local memory
+          const int ne = set ? p.n[1] : p.n[0];
+          if (c >= (set ? p.ncomp[1] : p.ncomp[0]) || ne == 0) continue;
+          const double* offs = set ? p.off[1] : p.off[0];
+          double* outs = set ? p.out[1] : p.out[0];
+          const int q0 = set ? p.lo[1][box] : p.lo[0][box];
+          const int q1 = set ? p.hi[1][box] : p.hi[0][box];
+          for (int c0 = q0; c0 < q1; c0 += ORDER_CHUNK) {
+            const int n = min(ORDER_CHUNK, q1 - c0);
+            order_chunk<T, DIM, W>(a, offs, ne, c0, n, perm, ordtmp, ordcnt);
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+              const int pt = c0 + perm[i];
+              double x[DIM];
+#pragma unroll
+              for (int k = 0; k < DIM; k++) x[k] = offs[(size_t)k * ne + pt] * a.scale_d;
+              if constexpr (DERIV) {
+                T v[1 + DIM];
+                interp_grad_point<T, DIM, W>(a, B, x, v);
+                const int nc = set ? p.ncomp[1] : p.ncomp[0];
+                outs[(size_t)id * ne + pt] += (double)v[0];
+                if (nc > 1) {
+#pragma unroll
+                  for (int d = 0; d < DIM; d++)
+                    outs[((size_t)(1 + d) * p.nd + id) * ne + pt] += (double)v[1 + d];
+                }
+              } else {
+                const T v = interp_point<T, DIM, W>(a, B, x);
+                outs[((size_t)c * p.nd + id) * ne + pt] += (double)v;
+              }
+            }
+            __syncthreads();
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+}
+
+// Direct modal evaluation for boxes with few points (at most pmax points of
+// both evaluation sets together), one CTA per box:
+//   u(x) = Re sum_m w(m) L_m e^{i k_m . x},  w = 1 on the kz = 0 plane and 2
+// elsewhere (Hermitian half space).  The phase factors e^{i k x_d} of the
+// box's points are computed once (FP64 sincos, stored as T, point index
+// fastest).  Mode rows (kx, ky) are summed over the last dimension.  Lanes
+// are (point, row subgroup) pairs for up to 32 points at a time, so a thread
+// accumulates one point over many rows in registers and the lanes of a warp
+// read at most 32/npoints distinct expansion rows per load; the partials of
+// all threads are added once per box in FP64.
+template <typename T, int DIM>
+__global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal(PWArgs<T> a, EvalPtrs<T> p,
+                                                              int pmax) {
+  constexpr int NHS = DIM * (DIM + 1) / 2, NCM = 1 + DIM + NHS;
+  constexpr int NW = MODAL_THREADS / 32;
+  const Geo& g = a.g;
+  const int K = g.K, NF = 2 * K + 1, NH = K + 1, NE = DIM * NF;
+  const int nrows = g.nexp / NH;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* red = reinterpret_cast<double*>(smem_raw);        // [NW][32][NCM]
+  T* E = reinterpret_cast<T*>(red + (size_t)NW * 32 * NCM);  // [NE][pmax] complex
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int bi = blockIdx.x; bi < p.nbox; bi += gridDim.x) {
+    const int e = p.boxes[bi];
+    const int box = p.eval_box[e];
+    const int n0 = p.n[0] > 0 && p.ncomp[0] > 0 ? p.hi[0][box] - p.lo[0][box] : 0;
+    const int n1 = p.n[1] > 0 && p.ncomp[1] > 0 ? p.hi[1][box] - p.lo[1][box] : 0;
+    const int np = n0 + n1;  // <= pmax by the box split
+    const int ncmax = max(n0 ? p.ncomp[0] : 0, n1 ? p.ncomp[1] : 0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < np * NE; i += blockDim.x) {
+      const int r = i / np, pi = i - r * np, d = r / NF, k = r - d * NF - K;
+      const int set = pi < n0 ? 0 : 1;
+      const int pt = set ? p.lo[1][box] + pi - n0 : p.lo[0][box] + pi;
+      const double* offs = set ? p.off[1] : p.off[0];
+      const int ne = set ? p.n[1] : p.n[0];
+      const double x = offs[(size_t)d * ne + pt] * a.scale_d;
+      double sn, cs;
+      sincos(x * (double)k, &sn, &cs);
+      E[2 * ((size_t)r * pmax + pi)] = (T)cs;
+      E[2 * ((size_t)r * pmax + pi) + 1] = (T)sn;
+    }
+    __syncthreads();
+    for (int id = 0; id < p.nd; id++) {
+      const T* L = p.loc + ((size_t)e * p.nd + id) * 2 * g.nexp;
+      // one row partition for every point of the box, so that equal points
+      // (a source that is also a target) get bitwise equal sums
+      const int nsub = 32 / max(1, min(32, np));
+      for (int p0 = 0; p0 < np; p0 += 32) {
+        const int npg = min(32, np - p0);
+        const int pi = p0 + lane % npg, sub = lane / npg;
+        const bool act = sub < nsub;
+        const T* Ex = E + 2 * (size_t)pi;  // + 2 * pmax * r for row r of E
+        const T* El = E + 2 * ((size_t)((DIM - 1) * NF + K) * pmax + pi);
+        T v[NCM];
+#pragma unroll
+        for (int c = 0; c < NCM; c++) v[c] = T(0);
+        if (act) {
+          for (int r = warp * nsub + sub; r < nrows; r += NW * nsub) {
+            int ki[3] = {0, 0, 0};
+            if (DIM == 3) {
+              ki[0] = r / NF;
+              ki[1] = r - ki[0] * NF;
+            } else if (DIM == 2) {
+              ki[0] = r;
+            }
+            const T* Lr = L + 2 * (size_t)r * NH;
+            T s0r = T(0), s0i = T(0), s1r = T(0), s1i = T(0), s2r = T(0), s2i = T(0);
+#pragma unroll 4
+            for (int kz = 0; kz < NH; kz++) {
+              const T w = kz == 0 ? T(1) : T(2);
+              const T lr = __ldg(Lr + 2 * kz) * w, li = __ldg(Lr + 2 * kz + 1) * w;
+              const T er = El[2 * (size_t)kz * pmax], ei = El[2 * (size_t)kz * pmax + 1];
+              const T tr = lr * er - li * ei, ti = lr * ei + li * er;
+              s0r += tr;
+              s0i += ti;
+              if (ncmax > 1) {
+                const T t = a.ts[K + kz];
+                s1r += t * tr;
+                s1i += t * ti;
+                if (ncmax > 1 + DIM) {
+                  s2r += t * t * tr;
+                  s2i += t * t * ti;
+                }
+              }
+            }
+            T pr = T(1), pim = T(0);  // phase of the row in the other dimensions
+#pragma unroll
+            for (int d = 0; d < DIM - 1; d++) {
+              const size_t o = 2 * (size_t)(d * NF + ki[d]) * pmax;
+              const T cr = Ex[o], ci = Ex[o + 1];
+              const T nr = pr * cr - pim * ci;
+              pim = pr * ci + pim * cr;
+              pr = nr;
+            }
+            const T t0r = pr * s0r - pim * s0i, t0i = pr * s0i + pim * s0r;
+            v[0] += t0r;
+            if (ncmax > 1) {
+              const T t1r = pr * s1r - pim * s1i, t1i = pr * s1i + pim * s1r;
+#pragma unroll
+              for (int d = 0; d < DIM - 1; d++) v[1 + d] -= t0i * a.ts[ki[d]];
+              v[DIM] -= t1i;
+              if (ncmax > 1 + DIM) {
+                const T t2r = pr * s2r - pim * s2i;
+#pragma unroll
+                for (int hm = 0; hm < NHS; hm++) {
+                  int pp, qq;
+                  if (DIM == 1) { pp = 0; qq = 0; }
+                  else if (DIM == 2) { pp = (hm == 2) ? 1 : 0; qq = (hm == 0) ? 0 : 1; }
+                  else { pp = hm < 3 ? hm : (hm < 5 ? 0 : 1); qq = hm < 3 ? hm : (hm == 3 ? 1 : 2); }
+                  const bool lp = pp == DIM - 1, lq = qq == DIM - 1;
+                  T h;
+                  if (lp && lq) h = t2r;
+                  else if (lp) h = t1r * a.ts[sel3(ki, qq)];
+                  else if (lq) h = t1r * a.ts[sel3(ki, pp)];
+                  else h = t0r * a.ts[sel3(ki, pp)] * a.ts[sel3(ki, qq)];
+                  v[1 + DIM + hm] -= h;
+                }
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < NCM; c++) red[((size_t)warp * 32 + lane) * NCM + c] = (double)v[c];
+        __syncthreads();
+        const double s1 = (double)a.inv_sqd0, s2 = s1 * s1;
+        for (int i = threadIdx.x; i < npg * NCM; i += blockDim.x) {
+          const int q = i / NCM, c = i - q * NCM, pj = p0 + q;
+          const int set = pj < n0 ? 0 : 1;
+          if (c >= (set ? p.ncomp[1] : p.ncomp[0])) continue;
+          double v2 = 0;
+          for (int w = 0; w < NW; w++)
+            for (int sb = 0; sb < nsub; sb++) v2 += red[((size_t)w * 32 + sb * npg + q) * NCM + c];
+          v2 *= c == 0 ? 1.0 : (c <= DIM ? s1 : s2);
+          const int ne = set ? p.n[1] : p.n[0];
+          const int pt = set ? p.lo[1][box] + pj - n0 : p.lo[0][box] + pj;
+          double* outs = set ? p.out[1] : p.out[0];
+          outs[((size_t)c * p.nd + id) * ne + pt] += v2;
+        }
+        __syncthreads();
+      }
+    }
+  }
+}
+
+// box partition by evaluation-point count
+__global__ void k_eval_split(int n_eval, const int* __restrict__ eval_box, const int* __restrict__ lo0,
+                             const int* __restrict__ hi0, const int* __restrict__ lo1,
+                             const int* __restrict__ hi1, int thr, int* __restrict__ big,
+                             unsigned long long* __restrict__ cnt) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_eval; e += gridDim.x * blockDim.x) {
+    int b = eval_box[e];
+    int n = (lo0 ? hi0[b] - lo0[b] : 0) + (lo1 ? hi1[b] - lo1[b] : 0);
+    big[e] = n > thr ? 1 : 0;
+    atomicAdd(&cnt[n > thr ? 0 : 1], (unsigned long long)n);
+  }
+}
+__global__ void k_split_fill(int n, const int* __restrict__ f, const int* __restrict__ pos,
+                             int* __restrict__ big_list, int* __restrict__ small_list) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    if (f[e]) big_list[pos[e]] = e;
+    else small_list[e - pos[e]] = e;
+  }
+}
+
+template <typename T, int DIM, int W, bool DERIV>
+int launch_eval_k(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t s) {
+  size_t fix = fixed_smem(a, W, 2);
+  size_t need = fix + sizeof(T) * (size_t)a.g.bufsz;
+  int grid = std::max(1, std::min(ep.nbox, kSMs));
+  bool gb = need > (size_t)MAXSMEM;
+  if (gb) {
+    gs.alloc((size_t)grid * a.g.bufsz, s);
+    a.gscratch = gs;
+  }
+  size_t sm = gb ? fix : need;
+  if (gb) {
+    auto k = k_eval_comp<T, DIM, W, true, DERIV>;
+    set_smem(k, sm);
+    k<<<grid, PW_THREADS, sm, s>>>(a, ep);
+  } else {
+    auto k = k_eval_comp<T, DIM, W, false, DERIV>;
+    set_smem(k, sm);
+    k<<<grid, PW_THREADS, sm, s>>>(a, ep);
+  }
+  FGT_LAUNCH_CHECK();
+  return 1;
+}
+
+// deriv: gradients through the kernel derivative (widths 8..16 only)
+template <typename T, int DIM, int W>
+int launch_eval(PWArgs<T>& a, const EvalPtrs<T>& ep, bool deriv, DBuf<T>& gs, cudaStream_t s) {
+  if constexpr (W >= 8) {
+    if (deriv) return launch_eval_k<T, DIM, W, true>(a, ep, gs, s);
+  }
+  FGT_REQUIRE(!deriv, FGT_ERR_UNSUPPORTED, "derivative evaluation needs a kernel width >= 8");
+  return launch_eval_k<T, DIM, W, false>(a, ep, gs, s);
+}
+
+template <typename T, int DIM>
+int eval_w(int w, PWArgs<T>& a, const EvalPtrs<T>& ep, bool deriv, DBuf<T>& gs, cudaStream_t s) {
+  switch (w) {
+    case 6: return launch_eval<T, DIM, 6>(a, ep, deriv, gs, s);
+    case 8: return launch_eval<T, DIM, 8>(a, ep, deriv, gs, s);
+    case 10: return launch_eval<T, DIM, 10>(a, ep, deriv, gs, s);
+    case 12: return launch_eval<T, DIM, 12>(a, ep, deriv, gs, s);
+    case 14: return launch_eval<T, DIM, 14>(a, ep, deriv, gs, s);
+    default: return launch_eval<T, DIM, 16>(a, ep, deriv, gs, s);
+  }
+}
+template <typename T>
+int eval_dim(int dim, int w, PWArgs<T>& a, const EvalPtrs<T>& ep, bool deriv, DBuf<T>& gs,
+             cudaStream_t s) {
+  if (dim == 1) return eval_w<T, 1>(w, a, ep, deriv, gs, s);
+  if (dim == 2) return eval_w<T, 2>(w, a, ep, deriv, gs, s);
+  return eval_w<T, 3>(w, a, ep, deriv, gs, s);
+}
+
+}  // namespace
+
+template <typename T>
+int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D,
+            const EvalSet<T>& e0, const EvalSet<T>& e1, int small_eval, PWWork* work,
+            cudaStream_t s) {
+  // both evaluation sets (sources, targets) share the grid of every box
+  const bool u0 = e0.pgh > 0 && e0.n > 0, u1 = e1.pgh > 0 && e1.n > 0;
+  if (!(u0 || u1) || L.n_eval <= 0) return 0;
+  const int pgh_max = std::max(u0 ? e0.pgh : 0, u1 ? e1.pgh : 0);
+  // Grids of the evaluation: potential only (width w); potential and
+  // gradient from one grid through the kernel derivative, whose aliasing
+  // error at width w+2 is below that of the potential at width w; one grid
+  // per output component (pot, grad_k, hess_kl) at width w when hessians are
+  // requested or w+2 exceeds the widest kernel.
+  const bool deriv = pgh_max == 2 && P.w + 2 <= 16;
+  const int mode = deriv ? 1 : 2;
+  PWParams Pe = P;
+  if (deriv) pw_grid(Pe, P.w + 2);
+  PWArgs<T> a;
+  DevTables<T> tb;
+  make_args<T>(Pe, a, tb, s, false);
+  int launches = 0;
+  // boxes with at most thr evaluation points use the modal sums; thr is
+  // capped by the modal kernel's shared memory (per point: FP64 partials of
+  // every warp and the phase factors)
+  const int ncm = 1 + P.dim + P.dim * (P.dim + 1) / 2;
+  const size_t modal_fix = sizeof(double) * MODAL_THREADS * ncm;
+  const size_t modal_pt = sizeof(T) * 2 * (size_t)P.dim * (2 * P.K + 1);
+  const int thr = std::min(small_eval >= 0 ? small_eval : (P.dim == 3 ? 48 : (P.dim == 2 ? 8 : 4)),
+                           (int)((MAXSMEM - modal_fix) / modal_pt));
+  DBuf<int> big(L.n_eval, s), pos(L.n_eval, s), tot(1, s);
+  DBuf<unsigned long long> cnt(2, s);
+  cnt.zero();
+  k_eval_split<<<grid_for(L.n_eval, 256), 256, 0, s>>>(
+      L.n_eval, L.eval_box, u0 ? e0.lo : nullptr, u0 ? e0.hi : nullptr, u1 ? e1.lo : nullptr,
+      u1 ? e1.hi : nullptr, thr, big, cnt);
+  FGT_LAUNCH_CHECK();
+  exclusive_scan_i32(big, pos, L.n_eval, tot, s);
+  int nbig = fetch_int(tot, s);
+  DBuf<int> lbig(std::max(nbig, 1), s), lsmall(std::max(L.n_eval - nbig, 1), s);
+  k_split_fill<<<grid_for(L.n_eval, 256), 256, 0, s>>>(L.n_eval, big, pos, lbig, lsmall);
+  FGT_LAUNCH_CHECK();
+  launches += 3;
+  int nh = P.dim * (P.dim + 1) / 2;
+  auto ncomp = [&](int pgh) { return pgh <= 0 ? 0 : 1 + (pgh >= 2 ? P.dim : 0) + (pgh >= 3 ? nh : 0); };
+  EvalPtrs<T> ep;
+  ep.loc = D.loc;
+  ep.eval_box = L.eval_box;
+  ep.nd = P.nd;
+  const EvalSet<T>* es[2] = {&e0, &e1};
+  bool us[2] = {u0, u1};
+  for (int i = 0; i < 2; i++) {
+    ep.off[i] = us[i] ? es[i]->off : nullptr;
+    ep.lo[i] = us[i] ? es[i]->lo : nullptr;
+    ep.hi[i] = us[i] ? es[i]->hi : nullptr;
+    ep.out[i] = us[i] ? es[i]->out : nullptr;
+    ep.n[i] = us[i] ? es[i]->n : 0;
+    ep.ncomp[i] = us[i] ? ncomp(es[i]->pgh) : 0;
+  }
+  ep.ncomp_max = std::max(ep.ncomp[0], ep.ncomp[1]);
+  DBuf<T> gs;
+  if (nbig > 0) {
+    ep.boxes = lbig;
+    ep.nbox = nbig;
+    launches += eval_dim<T>(P.dim, Pe.w, a, ep, deriv, gs, s);
+    if (work) work->n_nufft += nbig;
+  }
+  int nsmall = L.n_eval - nbig;
+  if (nsmall > 0) {
+    ep.boxes = lsmall;
+    ep.nbox = nsmall;
+    int grid = std::max(1, std::min(nsmall, kSMs * 8));
+    size_t sm = modal_fix + modal_pt * (size_t)std::max(thr, 1);
+    if (P.dim == 1) {
+      set_smem(k_eval_modal<T, 1>, sm);
+      k_eval_modal<T, 1><<<grid, MODAL_THREADS, sm, s>>>(a, ep, thr);
+    } else if (P.dim == 2) {
+      set_smem(k_eval_modal<T, 2>, sm);
+      k_eval_modal<T, 2><<<grid, MODAL_THREADS, sm, s>>>(a, ep, thr);
+    } else {
+      set_smem(k_eval_modal<T, 3>, sm);
+      k_eval_modal<T, 3><<<grid, MODAL_THREADS, sm, s>>>(a, ep, thr);
+    }
+    FGT_LAUNCH_CHECK();
+    launches++;
+  }
+  if (work) {
+    unsigned long long h[2] = {0, 0};
+    FGT_CUDA(cudaMemcpyAsync(h, cnt.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FGT_CUDA(cudaStreamSynchronize(s));
+    const double wd = pow((double)Pe.w, P.dim);
+    const double grids = mode == 2 ? ep.ncomp_max : 1;
+    // derivative mode: value and derivative sums along the last dimension
+    const double fl_pt = mode == 1 ? 4.0 * wd : 2.0 * wd * grids;
+    work->pts_nufft = (double)h[0];
+    work->pts_modal = (double)h[1];
+    work->flops_eval = (double)P.nd * (nbig * grids * pw_pass_flops(Pe) + (double)h[0] * fl_pt) +
+                       (double)P.nd * ep.ncomp_max * (double)h[1] * P.nexp * 8.0;
+    work->w_eval = Pe.w;
+    work->G_eval = Pe.G;
+  }
+  FGT_CUDA(cudaStreamSynchronize(s));  // tables lifetime
+  return launches;
+}
+
+template int pw_eval<float>(const PWParams&, const Tree&, const Lists&, const PWData<float>&,
+                            const EvalSet<float>&, const EvalSet<float>&, int, PWWork*,
+                            cudaStream_t);
+template int pw_eval<double>(const PWParams&, const Tree&, const Lists&, const PWData<double>&,
+                             const EvalSet<double>&, const EvalSet<double>&, int, PWWork*,
+                             cudaStream_t);
+
+}  // namespace fgt
