@@ -32,7 +32,7 @@ METRIC = "(N+M) pts/s, 3D N=1e7 eps=1e-6: mixed vs FP64 GPU path; rel err vs FP6
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="fgt", choices=["fgt", "reference"])
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -62,7 +62,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
 
@@ -226,8 +226,10 @@ def main():
         sample = ""
         cores = 1
         frac = None
+        # a bounded sample per step: the whole run stays within a few minutes
+        per_step = max(1.0, min(6.0, 90.0 / (a.warmup + a.steps)))
         for i in range(a.warmup + a.steps):
-            v, sample, cores, frac = cpu_reference(cfg, target_s=6.0, frac=frac)
+            v, sample, cores, frac = cpu_reference(cfg, target_s=per_step, frac=frac)
             if i >= a.warmup:
                 vals.append(v)
         v = float(np.median(vals))
@@ -279,10 +281,11 @@ def main():
         o.stats = C.pointer(st)
         return o
 
-    od = opts(1, True)
+    od = opts(1, False)  # timed steps: no per-phase events
+    odt = opts(1, True)  # phase breakdown, measured after the timed region
 
-    def step_dev():
-        F.pfgt_device(od, 1, 3, cfg["delta"], cfg["eps"], 0, 1.0, [0, 0, 0], N,
+    def step_dev(o=None):
+        F.pfgt_device(o or od, 1, 3, cfg["delta"], cfg["eps"], 0, 1.0, [0, 0, 0], N,
                       src_d.data_ptr(), 1, q_d.data_ptr(), 0, None, None, 2,
                       pot_d.data_ptr(), grad_d.data_ptr(), None, M, trg_d.data_ptr(), 2,
                       pt_d.data_ptr(), gt_d.data_ptr(), None)
@@ -307,7 +310,6 @@ def main():
 
     for _ in range(a.warmup):
         step_dev()
-    ms_phase = np.zeros(12)
     barrier()
     torch.cuda.synchronize()
     clk = ClockSampler(local)
@@ -317,15 +319,92 @@ def main():
     e0.record(stream)
     for _ in range(a.steps):
         step_dev()
-        ms_phase += np.array(st.ms[:12])
     e1.record(stream)
     torch.cuda.synchronize()
     clocks = clk.stop()
     barrier()
     ms = maxr(e0.elapsed_time(e1) / a.steps)
-    ms_phase /= a.steps
-    stats = st.as_dict()
     value = world * npts / (ms * 1e-3)
+    # per-phase CUDA-event times of the same call (untimed region)
+    ms_phase = np.zeros(12)
+    nph = 3
+    for _ in range(nph):
+        step_dev(odt)
+        ms_phase += np.array(st.ms[:12])
+    ms_phase /= nph
+    stats = st.as_dict()
+
+    # relative l2 error against an FP64 direct summation (all N sources, no
+    # cut-off) at a sample of evaluation points, computed on the GPU by the
+    # library's FP64 all-pairs kernel, independent of the fast path
+    def exact_at(pts_d):
+        n = pts_d.shape[0]
+        ep = torch.zeros((n, 1), dtype=torch.float64, device=dev)
+        eg = torch.zeros((n, 3, 1), dtype=torch.float64, device=dev)
+        L = F.lib()
+        f = L.fgt_direct_nomalloc
+        f.restype = C.c_int
+        f.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_int,
+                      C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                      C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                      C.c_void_p]
+        rc = f(1, 3, cfg["delta"], 1e300, None, N, src_d.data_ptr(), 1, q_d.data_ptr(), 0,
+               None, None, n, pts_d.data_ptr(), 2, ep.data_ptr(), eg.data_ptr(), None,
+               C.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError("fgt_direct_nomalloc failed: %d" % rc)
+        torch.cuda.synchronize()
+        return ep, eg
+
+    def rel(ref, got):
+        ref = ref.reshape(-1)
+        return float(torch.linalg.norm(ref - got.reshape(-1)) / torch.linalg.norm(ref))
+
+    acc = None
+    if not a.no_accuracy:
+        g = torch.Generator().manual_seed(7)
+        ns_s = min(1000, N)
+        ns_t = min(1000, M)
+        i_s = torch.randperm(N, generator=g)[:ns_s].to(dev)
+        i_t = torch.randperm(M, generator=g)[:ns_t].to(dev)
+        xs_p, xs_g = exact_at(src_d[i_s].contiguous())
+        xt_p, xt_g = exact_at(trg_d[i_t].contiguous())
+
+        def errs():
+            return {"pot": rel(torch.cat([xs_p, xt_p]), torch.cat([pot_d[i_s], pt_d[i_t]])),
+                    "grad": rel(torch.cat([xs_g, xt_g]), torch.cat([grad_d[i_s], gt_d[i_t]]))}
+
+        acc = {"reference": "FP64 direct sum over all sources (no cut-off), GPU all-pairs kernel",
+               "sample": f"{ns_s} sources + {ns_t} targets", "rel_l2": errs()}
+        # the FP64 GPU path side by side: time and error on the same workload
+        if world == 1 and a.precision == "mixed":
+            mixed_out = [t.clone() for t in (pot_d, grad_d, pt_d, gt_d)]
+            o64 = opts(1, False)
+            o64.precision = F.PREC_FP64
+            for _ in range(2):
+                step_dev(o64)
+            torch.cuda.synchronize()
+            k64 = max(2, min(a.steps, 5))
+            g0 = torch.cuda.Event(enable_timing=True)
+            g1 = torch.cuda.Event(enable_timing=True)
+            g0.record(stream)
+            for _ in range(k64):
+                step_dev(o64)
+            g1.record(stream)
+            torch.cuda.synchronize()
+            ms64 = g0.elapsed_time(g1) / k64
+            both = list(zip(mixed_out, (pot_d, grad_d, pt_d, gt_d)))
+            acc["fp64_path"] = {"value": npts / (ms64 * 1e-3), "unit": "pts/s",
+                                "ms_per_step": ms64, "steps": k64, "rel_l2": errs(),
+                                "mixed_speedup": ms64 / ms,
+                                "mixed_vs_fp64_rel_l2_all_points": {
+                                    "pot": rel(torch.cat([b.reshape(-1) for _, b in both[0::2]]),
+                                               torch.cat([m.reshape(-1) for m, _ in both[0::2]])),
+                                    "grad": rel(torch.cat([b.reshape(-1) for _, b in both[1::2]]),
+                                                torch.cat([m.reshape(-1) for m, _ in both[1::2]]))}}
+            del mixed_out, both
+            step_dev()  # leave the mixed results in the output buffers
+            torch.cuda.synchronize()
 
     # end to end through the public API with pinned host buffers
     e2e = None
@@ -373,7 +452,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if a.precision == "mixed" else "f64", "data": "synthetic",
             "config": config, "clocks": clocks, "e2e": e2e, "roofline": roof,
-            "cpu_baseline": cpu,
+            "cpu_baseline": cpu, "accuracy": acc,
             "gpu_launches": int(stats["n_kernel_launches"]) * a.steps,
             "phases_ms": {k: round(float(v), 4) for k, v in zip(
                 ["h2d", "tree", "sort_gather", "lists", "form", "translate", "eval", "direct",

@@ -39,12 +39,17 @@ constexpr int FCH = 8192;       // points sorted per round
 constexpr int PB = 8;           // points per warp batch
 constexpr int TP = 12;          // padded kernel row (TILE <= TP - 1)
 
+// twiddle tables, rounded up to 16 bytes (the tiled scratch follows)
+template <typename T>
+__host__ __device__ constexpr size_t tw_bytes16(int G, int K) {
+  return ((size_t)sizeof(T) * 2 * G * ((2 * K + 1) + (K + 1)) + 15) & ~(size_t)15;
+}
+// byte offset of the grid buffer in the tiled form kernel; every part is a
+// multiple of 16 bytes, so the kernel-row buffer is float4 aligned
 template <typename T>
 __host__ __device__ constexpr size_t tiled_offset(int G, int K) {
-  return ((size_t)sizeof(T) * 2 * G * ((2 * K + 1) + (K + 1)) + sizeof(int) * (2 * NBLK_MAX + 32) +
-          sizeof(int) * FCH + sizeof(unsigned short) * FCH +
-          sizeof(float) * (PW_THREADS / 32) * PB * 3 * TP + 15) &
-         ~(size_t)15;
+  return tw_bytes16<T>(G, K) + sizeof(int) * (2 * NBLK_MAX + 32) + sizeof(int) * FCH +
+         sizeof(unsigned short) * FCH + sizeof(float) * (PW_THREADS / 32) * PB * 3 * TP;
 }
 
 // Exclusive scan of cnt[0..n) into off[0..n) for n <= 2 * blockDim.x;
@@ -92,8 +97,9 @@ __device__ void spread_tiled(const PWArgs<T>& a, T* B, const double* __restrict_
                              const T* __restrict__ sq, const T* __restrict__ sr, bool is_q, int c0,
                              int n, int* cnt, int* boff, int* misc, int* tmp,
                              unsigned short* perm, T* rows) {
-  constexpr int TILE = TB + W - 1, NCOL = (TILE * TILE + 31) / 32;
+  constexpr int TILE = TB + W - 1, NCOL = (TILE * TILE + 31) / 32, NP2 = TP / 2;
   static_assert(TILE <= TP - 1, "tile row too long");
+  static_assert(std::is_same<T, float>::value, "tiled spreading is the FP32 path");
   const Geo& g = a.g;
   const int nbd = (g.G - W + 1 + TB - 1) / TB, nblk = nbd * nbd * nbd;
   for (int i = threadIdx.x; i < nblk; i += blockDim.x) cnt[i] = 0;
@@ -135,11 +141,12 @@ __device__ void spread_tiled(const PWArgs<T>& a, T* B, const double* __restrict_
     org[2] = (bi % nbd) * TB;
     org[1] = ((bi / nbd) % nbd) * TB;
     org[0] = (bi / (nbd * nbd)) * TB;
-    T acc[NCOL][TILE];
+    // z cells in pairs (packed FP32x2 FMAs); TILE <= TP - 1 cells in TP/2 pairs
+    float2 acc[NCOL][NP2];
 #pragma unroll
     for (int j = 0; j < NCOL; j++)
 #pragma unroll
-      for (int t = 0; t < TILE; t++) acc[j][t] = T(0);
+      for (int i = 0; i < NP2; i++) acc[j][i] = make_float2(0.f, 0.f);
     for (int k0 = 0; k0 < nb; k0 += PB) {
       const int np = min(PB, nb - k0);
       if (lane < 3 * PB) {
@@ -163,15 +170,21 @@ __device__ void spread_tiled(const PWArgs<T>& a, T* B, const double* __restrict_
       __syncwarp();
 #pragma unroll 1
       for (int pq = 0; pq < np; pq++) {
-        const T* row = R + pq * 3 * TP;
-        T rz[TP];
+        const float* row = R + pq * 3 * TP;
+        const float4* rv = reinterpret_cast<const float4*>(row + 2 * TP);
+        float2 rz[NP2];
 #pragma unroll
-        for (int t = 0; t < TP; t++) rz[t] = row[2 * TP + t];
+        for (int i = 0; i < NP2 / 2; i++) {
+          const float4 q4 = rv[i];
+          rz[2 * i] = make_float2(q4.x, q4.y);
+          rz[2 * i + 1] = make_float2(q4.z, q4.w);
+        }
 #pragma unroll
         for (int j = 0; j < NCOL; j++) {
-          const T v = row[cx[j]] * row[TP + cy[j]];
+          const float v = row[cx[j]] * row[TP + cy[j]];
+          const float2 vv = make_float2(v, v);
 #pragma unroll
-          for (int t = 0; t < TILE; t++) acc[j][t] = fma(v, rz[t], acc[j][t]);
+          for (int i = 0; i < NP2; i++) acc[j][i] = __ffma2_rn(vv, rz[i], acc[j][i]);
         }
       }
       __syncwarp();
@@ -180,10 +193,14 @@ __device__ void spread_tiled(const PWArgs<T>& a, T* B, const double* __restrict_
     for (int j = 0; j < NCOL; j++) {
       const int x = org[0] + cx[j], y = org[1] + cy[j];
       if (lane + 32 * j < TILE * TILE && x < g.G && y < g.G) {
-        T* col = B + x * g.str[0] + y * g.str[1] + org[2];
+        float* col = B + x * g.str[0] + y * g.str[1] + org[2];
 #pragma unroll
-        for (int t = 0; t < TILE; t++)
-          if (org[2] + t < g.G && acc[j][t] != T(0)) atomicAdd(col + t, acc[j][t]);
+        for (int i = 0; i < NP2; i++) {
+          const int t = 2 * i;
+          if (t < TILE && org[2] + t < g.G && acc[j][i].x != 0.f) atomicAdd(col + t, acc[j][i].x);
+          if (t + 1 < TILE && org[2] + t + 1 < g.G && acc[j][i].y != 0.f)
+            atomicAdd(col + t + 1, acc[j][i].y);
+        }
       }
     }
   }
@@ -203,7 +220,7 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
   int* ordcnt = ordtmp + ORDER_CHUNK;                        // 32
   unsigned short* perm = reinterpret_cast<unsigned short*>(ordcnt + 32);  // ORDER_CHUNK
   // tiled-spreading scratch
-  int* tcnt = reinterpret_cast<int*>(twh + 2 * G * NH);  // NBLK_MAX
+  int* tcnt = reinterpret_cast<int*>(smem_raw + tw_bytes16<T>(G, K));  // NBLK_MAX
   int* toff = tcnt + NBLK_MAX;                             // NBLK_MAX
   int* tmisc = toff + NBLK_MAX;                            // 32
   int* ttmp = tmisc + 32;                                  // FCH
@@ -453,10 +470,10 @@ void legendre(int nq, std::vector<double>& xq, std::vector<double>& wq) {
 }  // namespace
 
 // ------------------------------------------------------------------ host set-up
-void pw_grid(PWParams& P, int w) {
+void pw_grid(PWParams& P, int w, bool exact_w) {
   const double pi = 4.0 * atan(1.0);
   const int K = P.K, NF = 2 * K + 1;
-  w = supported_w(std::max(4, std::min(16, w)));
+  w = exact_w ? std::max(4, std::min(16, w)) : supported_w(std::max(4, std::min(16, w)));
   P.w = w;
   P.beta = 0.97 * pi * (1 - 1.0 / (2 * 2.0)) * w;
   P.halfw = w * P.dx / 2;

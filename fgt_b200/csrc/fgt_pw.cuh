@@ -38,7 +38,9 @@ struct PWParams {
 void pw_setup(PWParams& P, int dim, int nd, int npw, double pmax, int periodic_nodes,
               double bs0, double delta, double eps, double boxsize_cut, int spread_width);
 // (Re)computes the width-dependent grid of P (kernel width w cells).
-void pw_grid(PWParams& P, int w);
+// exact_w: use width w as given (odd widths of the FP32 derivative
+// evaluation); otherwise w is rounded up to an even supported width
+void pw_grid(PWParams& P, int w, bool exact_w = false);
 
 template <typename T>
 struct PWData {

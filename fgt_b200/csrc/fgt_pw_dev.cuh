@@ -11,13 +11,15 @@
 //
 // 3D FP32 spreading accumulates blocks of points in register tiles
 // (spread_tiled); the other spreading variants and the interpolation are
-// thread-per-point over a bank-balanced processing order of each box's
-// points (see order_chunk), so the 32 lanes of a warp touch 32 distinct
-// shared-memory banks at every stencil offset.
+// thread-per-point.  Interpolation visits each box's points sorted by
+// stencil base cell (order_cells: a warp reads few distinct addresses);
+// thread-per-point spreading and the periodic full grids use a bank-balanced
+// order (order_chunk: 32 distinct banks per stencil offset).
 #pragma once
 #include <math.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "fgt_pw.cuh"
@@ -95,7 +97,7 @@ __device__ __forceinline__ void pass_inplace(T* B, int nl, int nb, int SA, int S
         T tr[KG], ti[KG];
 #pragma unroll
         for (int j = 0; j < KG; j++) {
-          const int k = kg * KG + j;
+          const int k = kg + j * nkg;  // interleaved: neighbouring lanes, neighbouring modes
           const bool ok = k < nout;
           tr[j] = ok ? tw[2 * (l * nout + k)] : T(0);
           ti[j] = ok ? tw[2 * (l * nout + k) + 1] : T(0);
@@ -127,7 +129,7 @@ __device__ __forceinline__ void pass_inplace(T* B, int nl, int nb, int SA, int S
       if (!lact[g]) continue;
 #pragma unroll
       for (int j = 0; j < KG; j++) {
-        const int k = kg * KG + j;
+        const int k = kg + j * nkg;  // interleaved: neighbouring lanes, neighbouring modes
         if (k >= nout) break;
         if (MODE == 2) {
           B[base[g] + k * eout] = re[g][j];
@@ -156,14 +158,14 @@ __device__ __forceinline__ int pmod(int a, int n) {
   return c < 0 ? c + n : c;
 }
 
-// Stencil cell offsets (T units) along each dimension.  Lin: the sub-grid
-// case, cells base..base+W-1 (offsets fold into address immediates); Tab:
-// the periodic full grid, cells wrap modulo nf (one modulo per dimension).
 // ki[i] for a run-time i without demoting ki to local memory
 __device__ __forceinline__ int sel3(const int* ki, int i) {
   return i == 0 ? ki[0] : (i == 1 ? ki[1] : ki[2]);
 }
 
+// Stencil cell offsets (T units) along each dimension.  Lin: the sub-grid
+// case, cells base..base+W-1 (offsets fold into address immediates); Tab:
+// the periodic full grid, cells wrap modulo nf (one modulo per dimension).
 template <int DIM, int W>
 struct LinIdx {
   int o[DIM];
@@ -228,15 +230,29 @@ __device__ __forceinline__ void outer_cells(const IX& ix, const T* ph0, F&& body
   }
 }
 
-template <typename T, int DIM, int W, class IX>
-__device__ __forceinline__ T interp_cells(const T* B, const IX& ix, const T (*ph)[W]) {
+// Read-only view of a grid in dynamic shared memory by 32-bit element offset:
+// indexing the __shared__ array directly keeps every load a shared-space load
+// with the stencil offsets in the address immediate.  The global-memory grid
+// variants use a plain pointer, which supports the same + and [].
+template <typename T>
+struct SmemView {
+  int base;  // element offset from the start of dynamic shared memory
+  __device__ __forceinline__ SmemView operator+(int k) const { return SmemView{base + k}; }
+  __device__ __forceinline__ T operator[](int i) const {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    return reinterpret_cast<const T*>(smem_raw)[base + i];
+  }
+};
+
+template <typename T, int DIM, int W, class IX, class GV>
+__device__ __forceinline__ T interp_cells(const GV& B, const IX& ix, const T (*ph)[W]) {
   T acc = T(0);
   if constexpr (DIM == 1) {
 #pragma unroll
     for (int j = 0; j < W; j++) acc += B[ix.x(j)] * ph[0][j];
   } else if constexpr (DIM == 2) {
     outer_cells<T, W, 16>(ix, ph[0], [&](int xo, T p0) {
-      const T* bx = B + xo;
+      const auto bx = B + xo;
       T sy = T(0);
 #pragma unroll
       for (int jy = 0; jy < W; jy++) sy += bx[ix.z(jy)] * ph[1][jy];
@@ -244,11 +260,11 @@ __device__ __forceinline__ T interp_cells(const T* B, const IX& ix, const T (*ph
     });
   } else {
     outer_cells<T, W, 8>(ix, ph[0], [&](int xo, T p0) {
-      const T* bx = B + xo;
+      const auto bx = B + xo;
       T sx = T(0);
 #pragma unroll
       for (int jy = 0; jy < W; jy++) {
-        const T* bxy = bx + ix.y(jy);
+        const auto bxy = bx + ix.y(jy);
         T sy = T(0);
 #pragma unroll
         for (int jz = 0; jz < W; jz++) sy += bxy[ix.z(jz)] * ph[2][jz];
@@ -298,8 +314,8 @@ __device__ __forceinline__ int kernel_row(const PWArgs<T>& a, double x, T* phi) 
   return i0;
 }
 
-template <typename T, int DIM, int W>
-__device__ __forceinline__ T interp_point(const PWArgs<T>& a, const T* B, const double* x) {
+template <typename T, int DIM, int W, class GV>
+__device__ __forceinline__ T interp_point(const PWArgs<T>& a, const GV& B, const double* x) {
   T ph[DIM][W];
   int s[DIM];
 #pragma unroll
@@ -368,6 +384,41 @@ __device__ __forceinline__ void outer_cells2(const IX& ix, const T* p0, const T*
   }
 }
 
+// Value and derivative sums of one stencil line in the last dimension,
+// sum_j (B_j - bref) ph_j and sum_j (B_j - bref) dph_j.  FP32: cells in
+// pairs with packed FP32x2 add/FMA (two lanes of arithmetic per instruction
+// on sm_100), the last cell of an odd width alone.
+template <typename T, int W, class IX, class GV>
+__device__ __forceinline__ void line_sums(const GV& bl, const IX& ix, T bref, const T* ph,
+                                          const T* dph, T& s0, T& s1) {
+  if constexpr (std::is_same<T, float>::value) {
+    float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f);
+    const float2 nb = make_float2(-bref, -bref);
+#pragma unroll
+    for (int j = 0; j + 1 < W; j += 2) {
+      const float2 b = __fadd2_rn(make_float2(bl[ix.z(j)], bl[ix.z(j + 1)]), nb);
+      a0 = __ffma2_rn(b, make_float2(ph[j], ph[j + 1]), a0);
+      a1 = __ffma2_rn(b, make_float2(dph[j], dph[j + 1]), a1);
+    }
+    s0 = a0.x + a0.y;
+    s1 = a1.x + a1.y;
+    if constexpr (W % 2 == 1) {  // last cell of an odd width
+      const float b = bl[ix.z(W - 1)] - bref;
+      s0 += b * ph[W - 1];
+      s1 += b * dph[W - 1];
+    }
+  } else {
+    s0 = T(0);
+    s1 = T(0);
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+      const T b = bl[ix.z(j)] - bref;
+      s0 += b * ph[j];
+      s1 += b * dph[j];
+    }
+  }
+}
+
 // Potential and gradient of one grid at one point: v[0] = pot, v[1+d] = d/dx_d.
 // The sums run over B - Bref (Bref = the stencil's centre cell): the
 // derivative stencils sum to the derivative of the kernel's partition of
@@ -375,8 +426,8 @@ __device__ __forceinline__ void outer_cells2(const IX& ix, const T* p0, const T*
 // nothing, while the smaller summands keep the FP32 sums from cancelling
 // when the field varies slowly over the stencil.  The potential adds Bref
 // times the product of the kernel row sums back.
-template <typename T, int DIM, int W, class IX>
-__device__ __forceinline__ void interp_grad_cells(const T* B, const IX& ix, const T (*ph)[W],
+template <typename T, int DIM, int W, class IX, class GV>
+__device__ __forceinline__ void interp_grad_cells(const GV& B, const IX& ix, const T (*ph)[W],
                                                   const T (*dph)[W], T* v) {
   T ksum = T(1);
 #pragma unroll
@@ -401,14 +452,8 @@ __device__ __forceinline__ void interp_grad_cells(const T* B, const IX& ix, cons
     const T bref = B[ix.x(W / 2) + ix.z(W / 2)];
     T pot = T(0), gx = T(0), gy = T(0);
     outer_cells2<T, W, 16>(ix, ph[0], dph[0], [&](int xo, T px, T dpx) {
-      const T* bx = B + xo;
-      T s0 = T(0), s1 = T(0);
-#pragma unroll
-      for (int jy = 0; jy < W; jy++) {
-        const T b = bx[ix.z(jy)] - bref;
-        s0 += b * ph[1][jy];
-        s1 += b * dph[1][jy];
-      }
+      T s0, s1;
+      line_sums<T, W>(B + xo, ix, bref, ph[1], dph[1], s0, s1);
       pot += px * s0;
       gx += dpx * s0;
       gy += px * s1;
@@ -420,18 +465,12 @@ __device__ __forceinline__ void interp_grad_cells(const T* B, const IX& ix, cons
     const T bref = B[ix.x(W / 2) + ix.y(W / 2) + ix.z(W / 2)];
     T pot = T(0), gx = T(0), gy = T(0), gz = T(0);
     outer_cells2<T, W, 8>(ix, ph[0], dph[0], [&](int xo, T px, T dpx) {
-      const T* bx = B + xo;
+      const auto bx = B + xo;
       T t0 = T(0), t1 = T(0), t2 = T(0);
 #pragma unroll
       for (int jy = 0; jy < W; jy++) {
-        const T* bxy = bx + ix.y(jy);
-        T s0 = T(0), s1 = T(0);
-#pragma unroll
-        for (int jz = 0; jz < W; jz++) {
-          const T b = bxy[ix.z(jz)] - bref;
-          s0 += b * ph[2][jz];
-          s1 += b * dph[2][jz];
-        }
+        T s0, s1;
+        line_sums<T, W>(bx + ix.y(jy), ix, bref, ph[2], dph[2], s0, s1);
         t0 += ph[1][jy] * s0;
         t1 += dph[1][jy] * s0;
         t2 += ph[1][jy] * s1;
@@ -448,8 +487,8 @@ __device__ __forceinline__ void interp_grad_cells(const T* B, const IX& ix, cons
   }
 }
 
-template <typename T, int DIM, int W>
-__device__ __forceinline__ void interp_grad_point(const PWArgs<T>& a, const T* B, const double* x,
+template <typename T, int DIM, int W, class GV>
+__device__ __forceinline__ void interp_grad_point(const PWArgs<T>& a, const GV& B, const double* x,
                                                   T* v) {
   T ph[DIM][W], dph[DIM][W];
   int s[DIM];
@@ -500,6 +539,83 @@ __device__ __forceinline__ void order_chunk(const PWArgs<T>& a, const double* of
     perm[pos] = (unsigned short)i;
   }
   __syncthreads();
+}
+
+// Processing order of a chunk of points sorted by stencil base cell: a
+// counting sort over the (G-W+1)^DIM base cells of the sub-grid (nbins <=
+// NBINS_MAX).  Points that share a base cell become consecutive, so the lanes
+// of a warp read few distinct addresses at every stencil offset (equal
+// addresses are broadcast); distinct cells in a warp are neighbours in memory
+// and fall into different banks.  Bin k lives at slot (k % per) * blockDim +
+// k / per, so each thread's serial pass over its `per` consecutive bins reads
+// consecutive words across the block.  ws: 32 ints.
+constexpr int NBINS_MAX = 8192;
+
+template <typename T, int DIM, int W>
+__device__ __forceinline__ void order_cells(const PWArgs<T>& a, const double* off, int ne, int q0,
+                                            int n, int nbins, unsigned short* perm, int* tmp,
+                                            int* bins, int* ws) {
+  const Geo& g = a.g;
+  const int nb = g.G - W + 1, bd = blockDim.x, t = threadIdx.x;
+  const int per = (nbins + bd - 1) / bd;
+  auto slot = [&](int k) { return (k % per) * bd + k / per; };
+  for (int i = t; i < per * bd; i += bd) bins[i] = 0;
+  __syncthreads();
+  for (int i = t; i < n; i += bd) {
+    int key = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const double u = off[(size_t)d * ne + q0 + i] * a.scale_d * a.inv_dx_d;
+      int b = (int)ceil(u - a.hwdx_d) - g.l0;
+      b = b < 0 ? 0 : (b > g.G - W ? g.G - W : b);
+      key = key * nb + b;
+    }
+    const int r = atomicAdd(&bins[slot(key)], 1);
+    tmp[i] = key | (r << 13);
+  }
+  __syncthreads();
+  // exclusive scan over the bins in key order
+  int sum = 0;
+  for (int i = 0; i < per; i++) sum += bins[i * bd + t];
+  const int lane = t & 31, w = t >> 5, nw = bd >> 5;
+  int inc = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += u;
+  }
+  if (lane == 31) ws[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    const int x = lane < nw ? ws[lane] : 0;
+    int ix = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, ix, o);
+      if (lane >= o) ix += u;
+    }
+    if (lane < nw) ws[lane] = ix - x;
+  }
+  __syncthreads();
+  int ex = ws[w] + inc - sum;
+  for (int i = 0; i < per; i++) {
+    const int c = bins[i * bd + t];
+    bins[i * bd + t] = ex;
+    ex += c;
+  }
+  __syncthreads();
+  for (int i = t; i < n; i += bd) {
+    const int v = tmp[i];
+    perm[bins[slot(v & (NBINS_MAX - 1))] + (v >> 13)] = (unsigned short)i;
+  }
+  __syncthreads();
+}
+
+// byte offset of the grid buffer in the evaluation kernel: the ordering
+// scratch of order_offset, then the cell-order bins and scan workspace
+template <typename T>
+__host__ __device__ constexpr size_t eval_offset(int G, int K) {
+  return order_offset<T>(G, K) + sizeof(int) * (NBINS_MAX + 32);
 }
 
 template <typename T>

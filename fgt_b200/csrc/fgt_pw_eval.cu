@@ -25,6 +25,7 @@ struct EvalPtrs {
   double* out[2];
   int n[2], ncomp[2];
   int nd, ncomp_max;
+  int cell_bins;  // base cells of the sub-grid for the cell order, 0: bank-class order
 };
 
 // component factor (complex) of evaluation component c at mode ki[]
@@ -125,8 +126,15 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<
   int* ordtmp = reinterpret_cast<int*>(tih + 2 * NH * G);
   int* ordcnt = ordtmp + ORDER_CHUNK;
   unsigned short* perm = reinterpret_cast<unsigned short*>(ordcnt + 32);
+  int* bins = reinterpret_cast<int*>(smem_raw + order_offset<T>(G, K));  // NBINS_MAX
+  int* bws = bins + NBINS_MAX;                                            // 32
   T* B = GB ? a.gscratch + (size_t)blockIdx.x * g.bufsz
-            : reinterpret_cast<T*>(smem_raw + order_offset<T>(G, K));
+            : reinterpret_cast<T*>(smem_raw + eval_offset<T>(G, K));
+  // interpolation reads: shared-space view of the grid (pointer for GB)
+  const auto BV = [&]() {
+    if constexpr (GB) return static_cast<const T*>(B);
+    else return SmemView<T>{(int)(eval_offset<T>(G, K) / sizeof(T))};
+  }();
   load_tw(tif, a.tif, 2 * NF * G);
   load_tw(tih, a.tih, 2 * NH * G);
   __syncthreads();
@@ -148,7 +156,10 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<
           const int q1 = set ? p.hi[1][box] : p.hi[0][box];
           for (int c0 = q0; c0 < q1; c0 += ORDER_CHUNK) {
             const int n = min(ORDER_CHUNK, q1 - c0);
-            order_chunk<T, DIM, W>(a, offs, ne, c0, n, perm, ordtmp, ordcnt);
+            if (p.cell_bins > 0)
+              order_cells<T, DIM, W>(a, offs, ne, c0, n, p.cell_bins, perm, ordtmp, bins, bws);
+            else
+              order_chunk<T, DIM, W>(a, offs, ne, c0, n, perm, ordtmp, ordcnt);
             for (int i = threadIdx.x; i < n; i += blockDim.x) {
               const int pt = c0 + perm[i];
               double x[DIM];
@@ -156,7 +167,7 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<
               for (int k = 0; k < DIM; k++) x[k] = offs[(size_t)k * ne + pt] * a.scale_d;
               if constexpr (DERIV) {
                 T v[1 + DIM];
-                interp_grad_point<T, DIM, W>(a, B, x, v);
+                interp_grad_point<T, DIM, W>(a, BV, x, v);
                 const int nc = set ? p.ncomp[1] : p.ncomp[0];
                 outs[(size_t)id * ne + pt] += (double)v[0];
                 if (nc > 1) {
@@ -165,7 +176,7 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<
                     outs[((size_t)(1 + d) * p.nd + id) * ne + pt] += (double)v[1 + d];
                 }
               } else {
-                const T v = interp_point<T, DIM, W>(a, B, x);
+                const T v = interp_point<T, DIM, W>(a, BV, x);
                 outs[((size_t)c * p.nd + id) * ne + pt] += (double)v;
               }
             }
@@ -345,10 +356,17 @@ __global__ void k_split_fill(int n, const int* __restrict__ f, const int* __rest
 
 template <typename T, int DIM, int W, bool DERIV>
 int launch_eval_k(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t s) {
-  size_t fix = fixed_smem(a, W, 2);
+  size_t fix = eval_offset<T>(a.g.G, a.g.K);
   size_t need = fix + sizeof(T) * (size_t)a.g.bufsz;
   int grid = std::max(1, std::min(ep.nbox, kSMs));
   bool gb = need > (size_t)MAXSMEM;
+  EvalPtrs<T> epk = ep;
+  {  // cell order when the sub-grid's base cells fit the bins
+    const long nb = a.g.G - W + 1;
+    long nbins = 1;
+    for (int d = 0; d < DIM; d++) nbins *= nb;
+    epk.cell_bins = (!a.g.wrap && nb > 0 && nbins <= NBINS_MAX) ? (int)nbins : 0;
+  }
   if (gb) {
     gs.alloc((size_t)grid * a.g.bufsz, s);
     a.gscratch = gs;
@@ -357,11 +375,11 @@ int launch_eval_k(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t
   if (gb) {
     auto k = k_eval_comp<T, DIM, W, true, DERIV>;
     set_smem(k, sm);
-    k<<<grid, PW_THREADS, sm, s>>>(a, ep);
+    k<<<grid, PW_THREADS, sm, s>>>(a, epk);
   } else {
     auto k = k_eval_comp<T, DIM, W, false, DERIV>;
     set_smem(k, sm);
-    k<<<grid, PW_THREADS, sm, s>>>(a, ep);
+    k<<<grid, PW_THREADS, sm, s>>>(a, epk);
   }
   FGT_LAUNCH_CHECK();
   return 1;
@@ -370,18 +388,26 @@ int launch_eval_k(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t
 // deriv: gradients through the kernel derivative (widths 8..16 only)
 template <typename T, int DIM, int W>
 int launch_eval(PWArgs<T>& a, const EvalPtrs<T>& ep, bool deriv, DBuf<T>& gs, cudaStream_t s) {
-  if constexpr (W >= 8) {
-    if (deriv) return launch_eval_k<T, DIM, W, true>(a, ep, gs, s);
+  if constexpr (W % 2 == 1) {  // odd widths: FP32 derivative evaluation only
+    FGT_REQUIRE(deriv && sizeof(T) == 4, FGT_ERR_UNSUPPORTED, "odd kernel width outside the FP32 gradient path");
+    if constexpr (sizeof(T) == 4) return launch_eval_k<T, DIM, W, true>(a, ep, gs, s);
+    return 0;
+  } else {
+    if constexpr (W >= 8) {
+      if (deriv) return launch_eval_k<T, DIM, W, true>(a, ep, gs, s);
+    }
+    FGT_REQUIRE(!deriv, FGT_ERR_UNSUPPORTED, "derivative evaluation needs a kernel width >= 7");
+    return launch_eval_k<T, DIM, W, false>(a, ep, gs, s);
   }
-  FGT_REQUIRE(!deriv, FGT_ERR_UNSUPPORTED, "derivative evaluation needs a kernel width >= 8");
-  return launch_eval_k<T, DIM, W, false>(a, ep, gs, s);
 }
 
 template <typename T, int DIM>
 int eval_w(int w, PWArgs<T>& a, const EvalPtrs<T>& ep, bool deriv, DBuf<T>& gs, cudaStream_t s) {
   switch (w) {
     case 6: return launch_eval<T, DIM, 6>(a, ep, deriv, gs, s);
+    case 7: return launch_eval<T, DIM, 7>(a, ep, deriv, gs, s);
     case 8: return launch_eval<T, DIM, 8>(a, ep, deriv, gs, s);
+    case 9: return launch_eval<T, DIM, 9>(a, ep, deriv, gs, s);
     case 10: return launch_eval<T, DIM, 10>(a, ep, deriv, gs, s);
     case 12: return launch_eval<T, DIM, 12>(a, ep, deriv, gs, s);
     case 14: return launch_eval<T, DIM, 14>(a, ep, deriv, gs, s);
@@ -411,10 +437,13 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   // error at width w+2 is below that of the potential at width w; one grid
   // per output component (pot, grad_k, hess_kl) at width w when hessians are
   // requested or w+2 exceeds the widest kernel.
-  const bool deriv = pgh_max == 2 && P.w + 2 <= 16;
+  // FP32: width w+1 (its aliasing error, ~1e-7 at eps = 1e-6, stays below
+  // the FP32 rounding of the sums); FP64: w+2
+  const int wgrad = P.w + (sizeof(T) == 4 ? 1 : 2);
+  const bool deriv = pgh_max == 2 && wgrad <= 16;
   const int mode = deriv ? 1 : 2;
   PWParams Pe = P;
-  if (deriv) pw_grid(Pe, P.w + 2);
+  if (deriv) pw_grid(Pe, wgrad, true);
   PWArgs<T> a;
   DevTables<T> tb;
   make_args<T>(Pe, a, tb, s, false);
