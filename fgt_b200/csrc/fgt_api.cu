@@ -289,6 +289,7 @@ void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
   g.dmax = log(1.0 / c.eps) * c.delta;
   g.bs0 = t.boxsize[0];
   g.center = t.center;
+  g.level = t.level;
   double pairs = 0;
   launches += direct_near_field<T>(g, L, src, et, &pairs, s);
   launches += direct_near_field<T>(g, L, src, es, &pairs, s);

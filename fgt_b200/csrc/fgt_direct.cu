@@ -24,8 +24,26 @@ struct DArgs {
   const double *soff, *eoff;
   const T *q, *ds, *rn;
   const double* center;
+  const int* level;
+  double dmax_d;  // cut-off in FP64 for the box-pair test
   double* out;
 };
+
+// A list-1 source box lies entirely beyond the cut-off when the minimum
+// distance between the two boxes (centre offset dc, half sizes summed in hh)
+// exceeds sqrt(dmax): every one of its pairs fails the rr < dmax test, so the
+// box is skipped.  The relative margin covers the rounding of the FP32 pair
+// distances.
+template <int DIM>
+__device__ __forceinline__ bool box_beyond_cutoff(const double* dc, double hh, double dmax) {
+  double gap2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < DIM; k++) {
+    const double gk = fabs(dc[k]) - hh;
+    gap2 += gk > 0.0 ? gk * gk : 0.0;
+  }
+  return gap2 > dmax * (1.0 + 1e-6);
+}
 
 template <int DIM>
 struct HessIdx;
@@ -81,6 +99,7 @@ __global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
     double cT[DIM];
 #pragma unroll
     for (int k = 0; k < DIM; k++) cT[k] = a.center[(size_t)tb * DIM + k];
+    const int lT = a.level[tb];
     for (int li = a.l1_ptr[tb]; li < a.l1_ptr[tb + 1]; li++) {
       const int sb = a.l1_src[li];
       double dc[DIM];
@@ -95,6 +114,9 @@ __global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
         }
         dc[k] = (cs + sh) - cT[k];
       }
+      if (box_beyond_cutoff<DIM>(dc, 0.5 * a.bs0 * (ldexp(1.0, -lT) + ldexp(1.0, -a.level[sb])),
+                                 a.dmax_d))
+        continue;
       const int s0 = a.s_lo[sb], s1 = a.s_hi[sb];
       for (int base = s0; base < s1; base += 32) {
         const int j = base + lane;
@@ -248,6 +270,7 @@ __global__ void __launch_bounds__(DW * 32) k_direct32(DArgs<float> a) {
     double cT[DIM];
 #pragma unroll
     for (int k = 0; k < DIM; k++) cT[k] = a.center[(size_t)tb * DIM + k];
+    const int lT = a.level[tb];
     for (int li = a.l1_ptr[tb]; li < a.l1_ptr[tb + 1]; li++) {
       const int sb = a.l1_src[li];
       double dc[DIM];
@@ -262,6 +285,9 @@ __global__ void __launch_bounds__(DW * 32) k_direct32(DArgs<float> a) {
         }
         dc[k] = (cs + sh) - cT[k];
       }
+      if (box_beyond_cutoff<DIM>(dc, 0.5 * a.bs0 * (ldexp(1.0, -lT) + ldexp(1.0, -a.level[sb])),
+                                 a.dmax_d))
+        continue;
       const int s0 = a.s_lo[sb], s1 = a.s_hi[sb];
       for (int base = s0; base < s1; base += 32) {
         const int j = base + lane;
@@ -487,6 +513,8 @@ int direct_near_field(const DirectGeom& g, const Lists& L, const SourceSet<T>& s
   a.rn = src.rn;
   a.eoff = e.off;
   a.center = g.center;
+  a.level = g.level;
+  a.dmax_d = g.dmax;
   a.out = e.out;
   bool chg = src.q != nullptr, dip = src.ds != nullptr;
   for (int d0 = 0; d0 < g.nd; d0 += (g.nd == 1 ? 1 : 4)) {

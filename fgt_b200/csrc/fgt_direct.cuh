@@ -31,6 +31,7 @@ struct DirectGeom {
   int dim, nd, iperiod0, nboxes;
   double delta, dmax, bs0;
   const double* center;
+  const int* level;  // box levels (box size bs0 * 2^-level)
 };
 
 // Adds the list-1 interactions onto every point of `e`.  Returns the number
