@@ -42,6 +42,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-accuracy", action="store_true")
+    p.add_argument("--no-batch", action="store_true")
     p.add_argument("--profile-once", action="store_true",
                    help="one untimed step only (for ncu launch lists)")
     return p.parse_args()
@@ -442,6 +443,52 @@ def main():
         e2e = {"value": world * npts / (ms_e2e * 1e-3), "unit": "pts/s",
                "ms_per_step": ms_e2e, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
+    # batched workload: 512 independent instances through fgt_pfgt_batch
+    # (device-resident inputs), against a loop of single calls
+    batch = None
+    if rank == 0 and world == 1 and not a.no_batch:
+        inst = W.batch_instances()
+        L = F.lib()
+        L.fgt_pfgt_batch.restype = C.c_int
+        arr = (F.FgtInstance * len(inst))()
+        keepb = []
+        for x, kw in zip(arr, inst):
+            s_ = torch.from_numpy(kw["sources"]).to(dev)
+            q_ = torch.from_numpy(kw["charge"]).to(dev)
+            p_ = torch.empty((s_.shape[0], 1), dtype=torch.float64, device=dev)
+            b0, c0 = np.array([1.0]), np.zeros(3)
+            keepb.append((s_, q_, p_, b0, c0))
+            x.nd, x.dim, x.delta, x.eps, x.iperiod = 1, 3, kw["delta"], kw["eps"], 0
+            x.bs0, x.cen0 = F._ptr(b0), F._ptr(c0)
+            x.ns, x.sources, x.ifcharge, x.charge = s_.shape[0], s_.data_ptr(), 1, q_.data_ptr()
+            x.ifpgh, x.pot = 1, p_.data_ptr()
+        ob = F.FgtOpts()
+        L.fgt_opts_default(C.byref(ob))
+        ob.device_ptrs = 1
+        nb_pts = sum(x["sources"].shape[0] for x in inst)
+        L.fgt_pfgt_batch(C.byref(ob), len(inst), arr, 0)
+        torch.cuda.synchronize()
+        tb = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            rc = L.fgt_pfgt_batch(C.byref(ob), len(inst), arr, 0)
+            torch.cuda.synchronize()
+            tb.append(time.perf_counter() - t0)
+            if rc != 0:
+                raise RuntimeError("fgt_pfgt_batch failed: %d" % rc)
+        t0 = time.perf_counter()
+        L.fgt_pfgt_batch(C.byref(ob), len(inst), arr, 1)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter() - t0
+        batch = {"workload": "512 independent 3D instances, N log-uniform in [1e3, 1e5] "
+                             "(sources = targets), half uniform / half sphere, delta "
+                             "log-uniform in [1e-5, 1e-2], eps in {1e-3, 1e-6}, pot only",
+                 "points": nb_pts, "value": nb_pts / min(tb), "unit": "pts/s",
+                 "ms": 1e3 * min(tb), "timing": "host wall clock around the synchronous call",
+                 "sequential_value": nb_pts / t1,
+                 "note": "default worker count; sequential = the same call with one worker"}
+        del keepb
+
     roof = roofline(a, stats, ms_phase)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -452,7 +499,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if a.precision == "mixed" else "f64", "data": "synthetic",
             "config": config, "clocks": clocks, "e2e": e2e, "roofline": roof,
-            "cpu_baseline": cpu, "accuracy": acc,
+            "cpu_baseline": cpu, "accuracy": acc, "batch": batch,
             "gpu_launches": int(stats["n_kernel_launches"]) * a.steps,
             "phases_ms": {k: round(float(v), 4) for k, v in zip(
                 ["h2d", "tree", "sort_gather", "lists", "form", "translate", "eval", "direct",

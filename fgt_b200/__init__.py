@@ -73,9 +73,21 @@ class FgtError(RuntimeError):
 _lib = None
 
 # every symbol declared in include/fgt_b200.h
+class FgtInstance(C.Structure):
+    """Mirror of `fgt_instance` (include/fgt_b200.h)."""
+    _fields_ = [("nd", C.c_int), ("dim", C.c_int), ("delta", C.c_double), ("eps", C.c_double),
+                ("iperiod", C.c_int), ("bs0", C.c_void_p), ("cen0", C.c_void_p),
+                ("ns", C.c_int), ("sources", C.c_void_p), ("ifcharge", C.c_int),
+                ("charge", C.c_void_p), ("ifdipole", C.c_int), ("rnormal", C.c_void_p),
+                ("dipstr", C.c_void_p), ("ifpgh", C.c_int), ("pot", C.c_void_p),
+                ("grad", C.c_void_p), ("hess", C.c_void_p), ("nt", C.c_int),
+                ("targ", C.c_void_p), ("ifpghtarg", C.c_int), ("pottarg", C.c_void_p),
+                ("gradtarg", C.c_void_p), ("hesstarg", C.c_void_p), ("status", C.c_int)]
+
+
 EXPORTS = ["fgt_opts_default", "fgt_pfgt_c", "pfgt_", "pfgt_direct_", "fgt_last_status",
            "fgt_last_error", "fgt_version", "fgt_debug_tree_build", "fgt_debug_tree_get",
-           "fgt_debug_tree_free", "fgt_direct_nomalloc"]
+           "fgt_debug_tree_free", "fgt_direct_nomalloc", "fgt_pfgt_batch"]
 
 
 def lib():
@@ -173,6 +185,68 @@ def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None, rnorma
     if stats or timing:
         out["stats"] = st.as_dict()
     return out
+
+
+def pfgt_batch(instances, precision=PREC_AUTO, nworkers=0, ndiv=0, small_eval=-1):
+    """Many independent point FGTs in one call (host arrays).
+
+    `instances` is a list of dicts with the keyword arguments of `pfgt`
+    (nd, dim, delta, eps, iperiod, sources, charge, dipstr, rnormal, ifpgh,
+    targets, ifpghtarg, bs0, cen0).  Returns one result dict per instance, as
+    `pfgt` does; raises FgtError if any instance failed.
+    """
+    L = lib()
+    keep, outs = [], []
+    arr = (FgtInstance * len(instances))()
+    for x, (kw) in zip(arr, instances):
+        nd, dim = kw["nd"], kw["dim"]
+        src = _f64(kw["sources"], (-1, dim))
+        ns = src.shape[0]
+        trg = kw.get("targets")
+        trg = None if trg is None else _f64(trg, (-1, dim))
+        nt = 0 if trg is None else trg.shape[0]
+        ifpgh, ifpghtarg = kw.get("ifpgh", 1), kw.get("ifpghtarg", 0) if nt else 0
+        nhess = dim * (dim + 1) // 2
+        q = _f64(kw["charge"], (ns, nd)) if kw.get("charge") is not None else None
+        ds = _f64(kw["dipstr"], (ns, nd)) if kw.get("dipstr") is not None else None
+        rn = _f64(kw["rnormal"], (ns, dim)) if ds is not None else None
+        o = {"pot": np.zeros((ns, nd)) if ifpgh >= 1 else None,
+             "grad": np.zeros((ns, dim, nd)) if ifpgh >= 2 else None,
+             "hess": np.zeros((ns, nhess, nd)) if ifpgh >= 3 else None,
+             "pottarg": np.zeros((nt, nd)) if ifpghtarg >= 1 else None,
+             "gradtarg": np.zeros((nt, dim, nd)) if ifpghtarg >= 2 else None,
+             "hesstarg": np.zeros((nt, nhess, nd)) if ifpghtarg >= 3 else None}
+        b0 = np.array([float(kw.get("bs0", 1.0))])
+        c0 = np.zeros(3)
+        if kw.get("cen0") is not None:
+            c0[:dim] = np.asarray(kw["cen0"], dtype=np.float64)[:dim]
+        keep += [src, trg, q, ds, rn, b0, c0]
+        x.nd, x.dim, x.delta, x.eps = nd, dim, kw["delta"], kw["eps"]
+        x.iperiod = kw.get("iperiod", 0)
+        x.bs0, x.cen0 = _ptr(b0), _ptr(c0)
+        x.ns, x.sources = ns, _ptr(src)
+        x.ifcharge, x.charge = (1 if q is not None else 0), _ptr(q)
+        x.ifdipole, x.rnormal, x.dipstr = (1 if ds is not None else 0), _ptr(rn), _ptr(ds)
+        x.ifpgh, x.pot, x.grad, x.hess = ifpgh, _ptr(o["pot"]), _ptr(o["grad"]), _ptr(o["hess"])
+        x.nt, x.targ, x.ifpghtarg = nt, _ptr(trg), ifpghtarg
+        x.pottarg, x.gradtarg, x.hesstarg = _ptr(o["pottarg"]), _ptr(o["gradtarg"]), _ptr(o["hesstarg"])
+        outs.append((o, b0, c0, dim))
+    opts = FgtOpts()
+    L.fgt_opts_default(C.byref(opts))
+    opts.precision = precision
+    opts.ndiv = ndiv
+    opts.small_eval = small_eval
+    L.fgt_pfgt_batch.restype = C.c_int
+    rc = L.fgt_pfgt_batch(C.byref(opts), len(instances), arr, nworkers)
+    if rc != FGT_OK:
+        bad = [i for i, x in enumerate(arr) if x.status != FGT_OK]
+        raise FgtError(rc, f"instances {bad[:8]} failed")
+    res = []
+    for o, b0, c0, dim in outs:
+        r = {k: v for k, v in o.items() if v is not None}
+        r["bs0"], r["cen0"] = float(b0[0]), c0[:dim].copy()
+        res.append(r)
+    return res
 
 
 def pfgt_device(opts, nd, dim, delta, eps, iperiod, bs0, cen0, ns, src_ptr, ifcharge,

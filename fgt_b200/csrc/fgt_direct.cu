@@ -410,13 +410,137 @@ __global__ void __launch_bounds__(DW * 32) k_direct32(DArgs<float> a) {
   }
 }
 
+// FP32 near field with two evaluation points per lane (charges, potential
+// or potential + gradient, one density): a warp item is 64 points, lane l
+// holds points l and l+32 as the two halves of FP32x2 registers, and each
+// staged source feeds both through packed FP32x2 instructions, so the hi/lo
+// differences, r^2, exponent argument and the FMAs of both pairs cost one
+// instruction each.  Sources are staged negated and duplicated,
+// (-x_hi, -x_hi, -y_hi, -y_hi), (-z_hi, -z_hi, q, q), (-x_lo, -x_lo, -y_lo,
+// -y_lo), (-z_lo, -z_lo, 0, 0), so every operand pair is one 128-bit
+// broadcast load.  Same arithmetic per pair as k_direct32.
+template <int DIM, int PGH>
+__global__ void __launch_bounds__(DW * 32) k_direct32x2(DArgs<float> a) {
+  constexpr int NC = 1 + (PGH >= 2 ? DIM : 0);
+  __shared__ float4 sa[DW][32], sb4[DW][32], sc[DW][32], sd4[DW][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const float ce = a.dinv * 1.4426950408889634f;  // exp(-rr/delta) = 2^(-rr*ce)
+  const float2 nce = make_float2(-ce, -ce), nrf = make_float2(-a.rfac, -a.rfac);
+  for (int it = blockIdx.x * DW + warp; it < a.n_items; it += gridDim.x * DW) {
+    const int tb = a.item_box[it];
+    const int pA = a.item_lo[it] + lane, pB = pA + 32;
+    const int ehi = a.e_hi[tb];
+    const bool actA = pA < ehi, actB = pB < ehi;
+    float2 tx[3], txl[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      tx[k] = make_float2(0.f, 0.f);
+      txl[k] = make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int k = 0; k < DIM; k++) {
+      const double vA = actA ? a.eoff[(size_t)k * a.ne + pA] : 0.0;
+      const double vB = actB ? a.eoff[(size_t)k * a.ne + pB] : 0.0;
+      const float hA = (float)vA, hB = (float)vB;
+      tx[k] = make_float2(hA, hB);
+      txl[k] = make_float2((float)(vA - (double)hA), (float)(vB - (double)hB));
+    }
+    float2 acc[NC];
+    double accA[NC], accB[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      acc[c] = make_float2(0.f, 0.f);
+      accA[c] = 0.0;
+      accB[c] = 0.0;
+    }
+    double cT[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; k++) cT[k] = a.center[(size_t)tb * DIM + k];
+    const int lT = a.level[tb];
+    for (int li = a.l1_ptr[tb]; li < a.l1_ptr[tb + 1]; li++) {
+      const int sbx = a.l1_src[li];
+      double dc[DIM];
+#pragma unroll
+      for (int k = 0; k < DIM; k++) {
+        double cs = a.center[(size_t)sbx * DIM + k];
+        double sh = 0;
+        if (a.iperiod0 == 1) {  // pfgt_find_local_shift, src/pfgt/pfgt_direct.f:620-651
+          double dx = cT[k] - cs, dxp1 = dx - a.bs0, dxm1 = dx + a.bs0;
+          if (fabs(dx) > fabs(dxp1)) { dx = dxp1; sh = a.bs0; }
+          if (fabs(dx) > fabs(dxm1)) sh = -a.bs0;
+        }
+        dc[k] = (cs + sh) - cT[k];
+      }
+      if (box_beyond_cutoff<DIM>(dc, 0.5 * a.bs0 * (ldexp(1.0, -lT) + ldexp(1.0, -a.level[sbx])),
+                                 a.dmax_d))
+        continue;
+      const int s0 = a.s_lo[sbx], s1 = a.s_hi[sbx];
+      for (int base = s0; base < s1; base += 32) {
+        const int j = base + lane;
+        __syncwarp();
+        if (j < s1) {
+          float h[3] = {0, 0, 0}, l[3] = {0, 0, 0};
+#pragma unroll
+          for (int k = 0; k < DIM; k++) {
+            const double v = a.soff[(size_t)k * a.ns + j] + dc[k];
+            h[k] = (float)v;
+            l[k] = (float)(v - (double)h[k]);
+          }
+          const float qv = a.q[(size_t)a.d0 * a.ns + j];
+          sa[warp][lane] = make_float4(-h[0], -h[0], -h[1], -h[1]);
+          sb4[warp][lane] = make_float4(-h[2], -h[2], qv, qv);
+          sc[warp][lane] = make_float4(-l[0], -l[0], -l[1], -l[1]);
+          sd4[warp][lane] = make_float4(-l[2], -l[2], 0.f, 0.f);
+        }
+        __syncwarp();
+        const int cnt = min(32, s1 - base);
+#pragma unroll 4
+        for (int jj = 0; jj < cnt; jj++) {
+          const float4 A = sa[warp][jj], Bq = sb4[warp][jj], Cl = sc[warp][jj], Dl = sd4[warp][jj];
+          const float2 nh[3] = {make_float2(A.x, A.y), make_float2(A.z, A.w), make_float2(Bq.x, Bq.y)};
+          const float2 nl[3] = {make_float2(Cl.x, Cl.y), make_float2(Cl.z, Cl.w), make_float2(Dl.x, Dl.y)};
+          float2 dr[DIM], rr = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int k = 0; k < DIM; k++) {
+            dr[k] = __fadd2_rn(__fadd2_rn(tx[k], nh[k]), __fadd2_rn(txl[k], nl[k]));
+            rr = __ffma2_rn(dr[k], dr[k], rr);
+          }
+          const float2 arg = __fmul2_rn(rr, nce);
+          const float eA = rr.x < a.dmax ? fgt_ex2(arg.x) : 0.f;
+          const float eB = rr.y < a.dmax ? fgt_ex2(arg.y) : 0.f;
+          const float2 r = __fmul2_rn(make_float2(eA, eB), make_float2(Bq.z, Bq.w));
+          acc[0] = __fadd2_rn(acc[0], r);
+          if (PGH >= 2) {
+            // gnd_directcg, src/pfgt/pfgt_direct.f:98-140: grad += -2/delta (t - s) r
+            const float2 rg = __fmul2_rn(r, nrf);
+#pragma unroll
+            for (int k = 0; k < DIM; k++) acc[1 + k] = __ffma2_rn(dr[k], rg, acc[1 + k]);
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          accA[c] += (double)acc[c].x;
+          accB[c] += (double)acc[c].y;
+          acc[c] = make_float2(0.f, 0.f);
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      double* o = a.out + ((size_t)c * a.nd + a.d0) * a.ne;
+      if (actA) o[pA] += accA[c];
+      if (actB) o[pB] += accB[c];
+    }
+  }
+}
+
 __global__ void k_items_count(int nboxes, const int* __restrict__ l1_ptr, const int* __restrict__ lo,
                               const int* __restrict__ hi, const int* __restrict__ s_lo,
                               const int* __restrict__ s_hi, const int* __restrict__ l1_src,
-                              int* __restrict__ cnt, double* __restrict__ pairs) {
+                              int tpi, int* __restrict__ cnt, double* __restrict__ pairs) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nboxes; b += gridDim.x * blockDim.x) {
     int ne = hi[b] - lo[b], nl = l1_ptr[b + 1] - l1_ptr[b];
-    cnt[b] = (ne > 0 && nl > 0) ? (ne + 31) / 32 : 0;
+    cnt[b] = (ne > 0 && nl > 0) ? (ne + tpi - 1) / tpi : 0;
     if (pairs && ne > 0 && nl > 0) {
       double ns = 0;
       for (int i = l1_ptr[b]; i < l1_ptr[b + 1]; i++) ns += s_hi[l1_src[i]] - s_lo[l1_src[i]];
@@ -424,13 +548,13 @@ __global__ void k_items_count(int nboxes, const int* __restrict__ l1_ptr, const 
     }
   }
 }
-__global__ void k_items_fill(int nboxes, const int* __restrict__ cnt, const int* __restrict__ pos,
-                             const int* __restrict__ lo, int* __restrict__ ibox,
-                             int* __restrict__ ilo) {
+__global__ void k_items_fill(int nboxes, int tpi, const int* __restrict__ cnt,
+                             const int* __restrict__ pos, const int* __restrict__ lo,
+                             int* __restrict__ ibox, int* __restrict__ ilo) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nboxes; b += gridDim.x * blockDim.x)
     for (int c = 0; c < cnt[b]; c++) {
       ibox[pos[b] + c] = b;
-      ilo[pos[b] + c] = lo[b] + 32 * c;
+      ilo[pos[b] + c] = lo[b] + tpi * c;
     }
 }
 
@@ -470,11 +594,16 @@ int direct_near_field(const DirectGeom& g, const Lists& L, const SourceSet<T>& s
                       const EvalSet<T>& e, double* pairs, cudaStream_t s) {
   if (e.pgh <= 0 || e.n <= 0 || L.n_l1 <= 0) return 0;
   int nb = g.nboxes, launches = 0;
+  bool chg = src.q != nullptr, dip = src.ds != nullptr;
+  // two evaluation points per lane: FP32, charges only, pot or pot + grad, one density
+  const bool paired = sizeof(T) == 4 && chg && !dip && e.pgh <= 2 && g.nd == 1;
+  const int tpi = paired ? 64 : 32;
   DBuf<int> cnt(nb, s), pos(nb, s), tot(1, s);
   DBuf<double> dpairs(1, s);
   dpairs.zero();
   k_items_count<<<grid_for(nb, 128), 128, 0, s>>>(nb, L.l1_ptr, e.lo, e.hi, src.lo, src.hi,
-                                                   L.l1_src, cnt, pairs ? dpairs.get() : nullptr);
+                                                   L.l1_src, tpi, cnt,
+                                                   pairs ? dpairs.get() : nullptr);
   FGT_LAUNCH_CHECK();
   exclusive_scan_i32(cnt, pos, nb, tot, s);
   int n_items = fetch_int(tot, s);
@@ -487,7 +616,7 @@ int direct_near_field(const DirectGeom& g, const Lists& L, const SourceSet<T>& s
   launches += 2;
   if (n_items == 0) return launches;
   DBuf<int> ibox(n_items, s), ilo(n_items, s);
-  k_items_fill<<<grid_for(nb, 128), 128, 0, s>>>(nb, cnt, pos, e.lo, ibox, ilo);
+  k_items_fill<<<grid_for(nb, 128), 128, 0, s>>>(nb, tpi, cnt, pos, e.lo, ibox, ilo);
   FGT_LAUNCH_CHECK();
   launches++;
   DArgs<T> a;
@@ -516,7 +645,25 @@ int direct_near_field(const DirectGeom& g, const Lists& L, const SourceSet<T>& s
   a.level = g.level;
   a.dmax_d = g.dmax;
   a.out = e.out;
-  bool chg = src.q != nullptr, dip = src.ds != nullptr;
+  if constexpr (sizeof(T) == 4) {
+    if (paired) {
+      a.d0 = 0;
+      const int grid = std::max(1, std::min(ceil_div(n_items, DW), kSMs * 16));
+      const DArgs<float>& af = a;
+      if (g.dim == 1) {
+        if (e.pgh == 1) k_direct32x2<1, 1><<<grid, DW * 32, 0, s>>>(af);
+        else k_direct32x2<1, 2><<<grid, DW * 32, 0, s>>>(af);
+      } else if (g.dim == 2) {
+        if (e.pgh == 1) k_direct32x2<2, 1><<<grid, DW * 32, 0, s>>>(af);
+        else k_direct32x2<2, 2><<<grid, DW * 32, 0, s>>>(af);
+      } else {
+        if (e.pgh == 1) k_direct32x2<3, 1><<<grid, DW * 32, 0, s>>>(af);
+        else k_direct32x2<3, 2><<<grid, DW * 32, 0, s>>>(af);
+      }
+      FGT_LAUNCH_CHECK();
+      return launches + 1;
+    }
+  }
   for (int d0 = 0; d0 < g.nd; d0 += (g.nd == 1 ? 1 : 4)) {
     a.d0 = d0;
     if (g.nd == 1) dispatch_dim<T, 1>(a, g.dim, e.pgh, chg, dip, s);

@@ -96,6 +96,43 @@ int fgt_pfgt_c(const fgt_opts *opts, int nd, int dim, double delta, double eps,
                double *gradtarg, double *hesstarg);
 
 /*
+ * One instance of a batched call: the arguments of the reference pfgt
+ * (src/pfgt/pfgt.f:6-10) by value/pointer, plus its status on return.
+ */
+typedef struct fgt_instance {
+  int nd, dim;
+  double delta, eps;
+  int iperiod;
+  double *bs0, *cen0;
+  int ns;
+  const double *sources;
+  int ifcharge;
+  const double *charge;
+  int ifdipole;
+  const double *rnormal, *dipstr;
+  int ifpgh;
+  double *pot, *grad, *hess;
+  int nt;
+  const double *targ;
+  int ifpghtarg;
+  double *pottarg, *gradtarg, *hesstarg;
+  int status; /* out: FGT_OK or FGT_ERR_* of this instance */
+} fgt_instance;
+
+/*
+ * Many independent point FGTs (the batched workload of the reference's test
+ * scenarios: a loop of pfgt calls, src/pfgt/pfgt.f:6-409 each) in one call.
+ * Every instance gives the results of fgt_pfgt_c with the same options; the
+ * options' stream, stats and timing fields are ignored.  Instances run
+ * concurrently on `nworkers` host worker threads, each with its own stream
+ * and device workspace (<= 0: 12, at most the host's threads), largest
+ * instances first.  Returns when all instances are done: FGT_OK, or the
+ * first failing instance's status (each instance's own status is in its
+ * `status` field).
+ */
+int fgt_pfgt_batch(const fgt_opts *opts, int ninst, fgt_instance *inst, int nworkers);
+
+/*
  * gfortran-mangled drop-in for `call pfgt(...)` (src/pfgt/pfgt.f:6-10): all
  * 24 arguments by reference, no hidden string lengths.  The reference has no
  * error argument; on failure the requested outputs are NaN-filled and the
