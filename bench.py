@@ -443,6 +443,51 @@ def main():
         e2e = {"value": world * npts / (ms_e2e * 1e-3), "unit": "pts/s",
                "ms_per_step": ms_e2e, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
+    # reusable plan on the same workload: the tree, lists and sorted offsets
+    # are built once; each step is fgt_plan_execute with the charges
+    plan = None
+    if rank == 0 and world == 1:
+        L = F.lib()
+        L.fgt_plan_create.restype = C.c_void_p
+        L.fgt_plan_execute.restype = C.c_int
+        op = opts(1, False)
+        st_c = C.c_int(0)
+        b0p, c0p = C.c_double(1.0), np.zeros(3)
+        h = L.fgt_plan_create(C.byref(op), 1, 3, C.c_double(cfg["delta"]), C.c_double(cfg["eps"]),
+                              0, C.byref(b0p), c0p.ctypes.data_as(C.c_void_p), N,
+                              C.c_void_p(src_d.data_ptr()), M, C.c_void_p(trg_d.data_ptr()),
+                              C.byref(st_c))
+        if not h:
+            raise RuntimeError("fgt_plan_create failed: %d" % st_c.value)
+        ref_pot = pot_d.clone()
+        outp = [torch.empty_like(t) for t in (pot_d, grad_d, pt_d, gt_d)]
+
+        def step_plan():
+            rc = L.fgt_plan_execute(C.c_void_p(h), 1, C.c_void_p(q_d.data_ptr()), 0, None, None, 2,
+                                    C.c_void_p(outp[0].data_ptr()), C.c_void_p(outp[1].data_ptr()),
+                                    None, 2, C.c_void_p(outp[2].data_ptr()),
+                                    C.c_void_p(outp[3].data_ptr()), None)
+            if rc != 0:
+                raise RuntimeError("fgt_plan_execute failed: %d" % rc)
+
+        for _ in range(max(1, a.warmup)):
+            step_plan()
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(a.steps):
+            step_plan()
+        p1.record(stream)
+        torch.cuda.synchronize()
+        msp = p0.elapsed_time(p1) / a.steps
+        plan = {"ms_per_execute": msp, "value": npts / (msp * 1e-3), "unit": "pts/s",
+                "pot_rel_diff_vs_call": float(torch.linalg.norm(outp[0] - ref_pot) /
+                                              torch.linalg.norm(ref_pot)),
+                "note": "fgt_plan_execute on the same points (tree, lists, offsets reused)"}
+        L.fgt_plan_destroy(C.c_void_p(h))
+        del outp, ref_pot
+
     # batched workload: 512 independent instances through fgt_pfgt_batch
     # (device-resident inputs), against a loop of single calls
     batch = None
@@ -499,7 +544,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if a.precision == "mixed" else "f64", "data": "synthetic",
             "config": config, "clocks": clocks, "e2e": e2e, "roofline": roof,
-            "cpu_baseline": cpu, "accuracy": acc, "batch": batch,
+            "cpu_baseline": cpu, "accuracy": acc, "batch": batch, "plan": plan,
             "gpu_launches": int(stats["n_kernel_launches"]) * a.steps,
             "phases_ms": {k: round(float(v), 4) for k, v in zip(
                 ["h2d", "tree", "sort_gather", "lists", "form", "translate", "eval", "direct",

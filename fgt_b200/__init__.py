@@ -87,7 +87,8 @@ class FgtInstance(C.Structure):
 
 EXPORTS = ["fgt_opts_default", "fgt_pfgt_c", "pfgt_", "pfgt_direct_", "fgt_last_status",
            "fgt_last_error", "fgt_version", "fgt_debug_tree_build", "fgt_debug_tree_get",
-           "fgt_debug_tree_free", "fgt_direct_nomalloc", "fgt_pfgt_batch"]
+           "fgt_debug_tree_free", "fgt_direct_nomalloc", "fgt_pfgt_batch", "fgt_plan_create",
+           "fgt_plan_execute", "fgt_plan_destroy"]
 
 
 def lib():
@@ -247,6 +248,72 @@ def pfgt_batch(instances, precision=PREC_AUTO, nworkers=0, ndiv=0, small_eval=-1
         r["bs0"], r["cen0"] = float(b0[0]), c0[:dim].copy()
         res.append(r)
     return res
+
+
+class Plan:
+    """Reusable plan (fgt_plan_create/execute/destroy): the tree, lists and
+    sorted point offsets of fixed sources and targets kept on the device for
+    repeated evaluations with new strengths (host arrays)."""
+
+    def __init__(self, nd, dim, delta, eps, iperiod, sources, targets=None, bs0=1.0, cen0=None,
+                 precision=PREC_AUTO, ndiv=0, small_eval=-1):
+        L = lib()
+        L.fgt_plan_create.restype = C.c_void_p
+        L.fgt_plan_execute.restype = C.c_int
+        self.nd, self.dim = nd, dim
+        self._src = _f64(sources, (-1, dim))
+        self.ns = self._src.shape[0]
+        self._trg = None if targets is None else _f64(targets, (-1, dim))
+        self.nt = 0 if self._trg is None else self._trg.shape[0]
+        b0 = C.c_double(float(bs0))
+        c0 = np.zeros(3)
+        if cen0 is not None:
+            c0[:dim] = np.asarray(cen0, dtype=np.float64)[:dim]
+        o = FgtOpts()
+        L.fgt_opts_default(C.byref(o))
+        o.precision, o.ndiv, o.small_eval = precision, ndiv, small_eval
+        st = C.c_int(0)
+        self._h = L.fgt_plan_create(C.byref(o), nd, dim, C.c_double(delta), C.c_double(eps),
+                                    iperiod, C.byref(b0),
+                                    c0.ctypes.data_as(_dp), self.ns, _ptr(self._src), self.nt,
+                                    _ptr(self._trg), C.byref(st))
+        if not self._h:
+            raise FgtError(st.value, last_error())
+        self.bs0, self.cen0 = b0.value, c0[:dim].copy()
+
+    def execute(self, charge=None, dipstr=None, rnormal=None, ifpgh=1, ifpghtarg=0):
+        """Results of pfgt on the plan's points for these strengths (dict as `pfgt`)."""
+        L = lib()
+        nd, dim, ns, nt = self.nd, self.dim, self.ns, self.nt
+        nhess = dim * (dim + 1) // 2
+        q = _f64(charge, (ns, nd)) if charge is not None else None
+        ds = _f64(dipstr, (ns, nd)) if dipstr is not None else None
+        rn = _f64(rnormal, (ns, dim)) if ds is not None else None
+        ifpghtarg = ifpghtarg if nt else 0
+        out = {"pot": np.zeros((ns, nd)) if ifpgh >= 1 else None,
+               "grad": np.zeros((ns, dim, nd)) if ifpgh >= 2 else None,
+               "hess": np.zeros((ns, nhess, nd)) if ifpgh >= 3 else None,
+               "pottarg": np.zeros((nt, nd)) if ifpghtarg >= 1 else None,
+               "gradtarg": np.zeros((nt, dim, nd)) if ifpghtarg >= 2 else None,
+               "hesstarg": np.zeros((nt, nhess, nd)) if ifpghtarg >= 3 else None}
+        rc = L.fgt_plan_execute(C.c_void_p(self._h), 1 if q is not None else 0, _ptr(q),
+                                1 if ds is not None else 0, _ptr(rn), _ptr(ds), ifpgh,
+                                _ptr(out["pot"]), _ptr(out["grad"]), _ptr(out["hess"]), ifpghtarg,
+                                _ptr(out["pottarg"]), _ptr(out["gradtarg"]), _ptr(out["hesstarg"]))
+        if rc != FGT_OK:
+            raise FgtError(rc, last_error())
+        return {k: v for k, v in out.items() if v is not None}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fgt_plan_destroy(C.c_void_p(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def pfgt_device(opts, nd, dim, delta, eps, iperiod, bs0, cen0, ns, src_ptr, ifcharge,

@@ -144,10 +144,33 @@ struct Call {
   double *pot, *grad, *hess, *pott, *gradt, *hesst;  // device pointers
 };
 
-template <typename T>
-void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o, fgt_stats* st,
-              cudaStream_t s, Timer& tm) {
-  const int dim = c.dim, nd = c.nd, nhess = dim * (dim + 1) / 2;
+// Point-dependent part of a call: scalar set-up, tree, lists, sorted FP64
+// offsets of every point from its reference box centre, and the inverse leaf
+// permutations of the output reorder.  Independent of the strengths and of
+// the arithmetic type, so a plan can keep it across calls.
+struct Setup {
+  int dim = 0, nd = 0, iperiod = 0, ns = 0, nt = 0;
+  double delta = 0, eps = 0;
+  int npwlevel = 0, ndiv = 0, nlevels = 0, npw = 0, iperiod0 = 0, nlevend = 0;
+  double pmax = 0, bs0 = 0, cen0[FGT_MAXDIM] = {0, 0, 0};
+  bool periodic_nodes = false, do_pw = false;
+  Tree t;
+  Lists L;
+  DBuf<double> soff, toff;
+  DBuf<uint32_t> inv_s, inv_t;
+  int launches = 0;
+};
+
+void setup_geometry(Setup& u, const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
+                    cudaStream_t s, Timer& tm) {
+  const int dim = c.dim;
+  u.dim = dim;
+  u.nd = c.nd;
+  u.iperiod = c.iperiod;
+  u.ns = c.ns;
+  u.nt = c.nt;
+  u.delta = c.delta;
+  u.eps = c.eps;
   int launches = 0;
   // --- scalar set-up (pfgt.f:110-140)
   int npwlevel = 0;
@@ -160,9 +183,11 @@ void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
     *bs0_io = bs0;
     for (int k = 0; k < dim; k++) cen0_io[k] = cen0[k];
   }
+  u.bs0 = bs0;
+  for (int k = 0; k < dim; k++) u.cen0[k] = cen0[k];
   int ndiv = o.ndiv > 0 ? o.ndiv : (dim == 1 ? 20 : (dim == 2 ? 80 : 250));
   // --- tree (pts_tree_mem/build, pts_tree_sort)
-  Tree t;
+  Tree& t = u.t;
   tree_build(t, dim, c.iperiod, npwlevel, ndiv, bs0, cen0, c.src, c.ns, c.trg, c.nt, s);
   launches += 12 + 6 * t.nlevels;
   tm.mark(1);
@@ -206,23 +231,54 @@ void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
     do_pw = false;
     nlevend = 0;
   }
-  Lists L;
-  build_lists(t, npwlevel, iperiod0, nlevend, do_pw, L, s);
+  build_lists(t, npwlevel, iperiod0, nlevend, do_pw, u.L, s);
   launches += do_pw ? 8 : 2;
   tm.mark(3);
   // --- gather (dreorderf, fmmcommon2d.f:3-27) as offsets from reference boxes
-  DBuf<double> soff((size_t)c.ns * dim, s), toff((size_t)std::max(c.nt, 1) * dim, s);
-  DBuf<T> qs, dss, rns;
+  u.soff.alloc((size_t)c.ns * dim, s);
+  u.toff.alloc((size_t)std::max(c.nt, 1) * dim, s);
   k_gather_coords<double><<<grid_for(c.ns, 256), 256, 0, s>>>(c.src, c.ns, dim, t.isrc, t.src_ref,
-                                                          t.center, soff);
+                                                              t.center, u.soff);
   FGT_LAUNCH_CHECK();
   launches++;
   if (c.nt > 0) {
-    k_gather_coords<double><<<grid_for(c.nt, 256), 256, 0, s>>>(c.trg, c.nt, dim, t.itrg, t.trg_ref,
-                                                            t.center, toff);
+    k_gather_coords<double><<<grid_for(c.nt, 256), 256, 0, s>>>(c.trg, c.nt, dim, t.itrg,
+                                                                t.trg_ref, t.center, u.toff);
     FGT_LAUNCH_CHECK();
     launches++;
   }
+  // inverse leaf permutations for the output reorder
+  u.inv_s.alloc(std::max(c.ns, 1), s);
+  k_invert<<<grid_for(c.ns, 256), 256, 0, s>>>(t.isrc, c.ns, u.inv_s);
+  FGT_LAUNCH_CHECK();
+  launches++;
+  u.inv_t.alloc(std::max(c.nt, 1), s);
+  if (c.nt > 0) {
+    k_invert<<<grid_for(c.nt, 256), 256, 0, s>>>(t.itrg, c.nt, u.inv_t);
+    FGT_LAUNCH_CHECK();
+    launches++;
+  }
+  u.npwlevel = npwlevel;
+  u.ndiv = ndiv;
+  u.nlevels = nlevels;
+  u.npw = npw;
+  u.pmax = pmax;
+  u.iperiod0 = iperiod0;
+  u.periodic_nodes = periodic_nodes;
+  u.nlevend = nlevend;
+  u.do_pw = do_pw;
+  u.launches = launches;
+}
+
+// Strength-dependent part of a call on a prepared geometry.
+template <typename T>
+void execute(const Setup& u, const Call& c, const fgt_opts& o, fgt_stats* st, cudaStream_t s,
+             Timer& tm) {
+  const int dim = u.dim, nd = u.nd, nhess = dim * (dim + 1) / 2;
+  const Tree& t = u.t;
+  const Lists& L = u.L;
+  int launches = u.launches;
+  DBuf<T> qs, dss, rns;
   if (c.ifcharge) {
     qs.alloc((size_t)c.ns * nd, s);
     k_gather_vals<T><<<grid_for(c.ns, 256), 256, 0, s>>>(c.q, c.ns, nd, t.isrc, qs);
@@ -249,21 +305,21 @@ void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
   launches += 2;
   SourceSet<T> src;
   src.n = c.ns;
-  src.off = soff;
+  src.off = u.soff;
   src.q = c.ifcharge ? qs.get() : nullptr;
   src.ds = c.ifdipole ? dss.get() : nullptr;
   src.rn = c.ifdipole ? rns.get() : nullptr;
   src.lo = t.src_lo;
   src.hi = t.src_hi;
   EvalSet<T> es, et;
-  es.n = c.ns; es.pgh = c.ifpgh; es.off = soff; es.lo = t.src_lo; es.hi = t.src_hi; es.out = outs;
-  et.n = c.nt; et.pgh = c.ifpghtarg; et.off = toff; et.lo = t.trg_lo; et.hi = t.trg_hi; et.out = outt;
+  es.n = c.ns; es.pgh = c.ifpgh; es.off = u.soff; es.lo = t.src_lo; es.hi = t.src_hi; es.out = outs;
+  et.n = c.nt; et.pgh = c.ifpghtarg; et.off = u.toff; et.lo = t.trg_lo; et.hi = t.trg_hi; et.out = outt;
   tm.mark(2);
   // --- plane waves (pfgt.f:700-1073)
   PWWork work;
-  if (do_pw && L.n_eval > 0) {
+  if (u.do_pw && L.n_eval > 0) {
     PWParams P;
-    pw_setup(P, dim, nd, npw, pmax, periodic_nodes ? 1 : 0, t.boxsize[0], c.delta, c.eps,
+    pw_setup(P, dim, nd, u.npw, u.pmax, u.periodic_nodes ? 1 : 0, t.boxsize[0], c.delta, c.eps,
              t.boxsize[t.ncutoff], o.spread_width);
     PWData<T> D;
     PWWork* wk = st ? &work : nullptr;
@@ -283,7 +339,7 @@ void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
   DirectGeom g;
   g.dim = dim;
   g.nd = nd;
-  g.iperiod0 = iperiod0;
+  g.iperiod0 = u.iperiod0;
   g.nboxes = t.nboxes;
   g.delta = c.delta;
   g.dmax = log(1.0 / c.eps) * c.delta;
@@ -295,32 +351,25 @@ void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
   launches += direct_near_field<T>(g, L, src, es, &pairs, s);
   tm.mark(7);
   // --- back to input order
-  {
-    DBuf<uint32_t> inv(std::max(std::max(c.ns, c.nt), 1), s);
-    if (c.ifpgh >= 1) {
-      k_invert<<<grid_for(c.ns, 256), 256, 0, s>>>(t.isrc, c.ns, inv);
-      FGT_LAUNCH_CHECK();
-      k_gather_out<<<grid_for(c.ns, 256), 256, 0, s>>>(outs, c.ns, nd, dim, c.ifpgh, inv, c.pot,
-                                                       c.grad, c.hess);
-      FGT_LAUNCH_CHECK();
-      launches += 2;
-    }
-    if (c.ifpghtarg >= 1 && c.nt > 0) {
-      k_invert<<<grid_for(c.nt, 256), 256, 0, s>>>(t.itrg, c.nt, inv);
-      FGT_LAUNCH_CHECK();
-      k_gather_out<<<grid_for(c.nt, 256), 256, 0, s>>>(outt, c.nt, nd, dim, c.ifpghtarg, inv,
-                                                       c.pott, c.gradt, c.hesst);
-      FGT_LAUNCH_CHECK();
-      launches += 2;
-    }
+  if (c.ifpgh >= 1) {
+    k_gather_out<<<grid_for(c.ns, 256), 256, 0, s>>>(outs, c.ns, nd, dim, c.ifpgh, u.inv_s, c.pot,
+                                                     c.grad, c.hess);
+    FGT_LAUNCH_CHECK();
+    launches++;
+  }
+  if (c.ifpghtarg >= 1 && c.nt > 0) {
+    k_gather_out<<<grid_for(c.nt, 256), 256, 0, s>>>(outt, c.nt, nd, dim, c.ifpghtarg, u.inv_t,
+                                                     c.pott, c.gradt, c.hesst);
+    FGT_LAUNCH_CHECK();
+    launches++;
   }
   tm.mark(8);
   if (st) {
-    st->nlevels = nlevels;
+    st->nlevels = u.nlevels;
     st->nboxes = t.nboxes;
-    st->npwlevel = npwlevel;
-    st->npw = npw;
-    st->ndiv = ndiv;
+    st->npwlevel = u.npwlevel;
+    st->npw = u.npw;
+    st->ndiv = u.ndiv;
     st->n_form_boxes = L.n_form;
     st->n_eval_boxes = L.n_eval;
     st->n_eval_nufft = work.n_nufft;
@@ -342,9 +391,17 @@ void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
     st->n_translations = L.n_trans;
     st->near_pairs = pairs;
     st->n_kernel_launches = launches;
-    st->bs0 = bs0;
-    for (int k = 0; k < dim; k++) st->cen0[k] = cen0[k];
+    st->bs0 = u.bs0;
+    for (int k = 0; k < dim; k++) st->cen0[k] = u.cen0[k];
   }
+}
+
+template <typename T>
+void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o, fgt_stats* st,
+              cudaStream_t s, Timer& tm) {
+  Setup u;
+  setup_geometry(u, c, bs0_io, cen0_io, o, s, tm);
+  execute<T>(u, c, o, st, s, tm);
 }
 
 bool fault_requested(const char* what) {
@@ -462,6 +519,163 @@ int pfgt_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps
 
 }  // namespace fgt
 
+// A plan: the point-dependent part of pfgt (tree, lists, sorted offsets,
+// inverse permutations) kept on the device, in an arena the plan owns, for
+// repeated calls with new strengths on the same points.
+struct fgt_plan {
+  int device = 0;
+  int prec = FGT_PREC_MIXED;
+  fgt_opts o;
+  fgt::Arena* arena = nullptr;
+  fgt::Setup u;
+};
+
+namespace fgt {
+namespace {
+
+fgt_plan* plan_create_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps,
+                           int iperiod, double* bs0, double* cen0, int ns, const double* sources,
+                           int nt, const double* targ) {
+  fgt_opts o;
+  fgt_opts_default(&o);
+  if (opts_in) o = *opts_in;
+  FGT_REQUIRE(dim >= 1 && dim <= 3, FGT_ERR_ARG, "dim must be 1, 2 or 3");
+  FGT_REQUIRE(nd >= 1, FGT_ERR_ARG, "nd must be >= 1");
+  FGT_REQUIRE(delta > 0 && isfinite(delta), FGT_ERR_ARG, "delta must be positive");
+  FGT_REQUIRE(eps > 0 && eps < 1, FGT_ERR_ARG, "eps must lie in (0,1)");
+  FGT_REQUIRE(ns >= 1, FGT_ERR_ARG, "ns must be >= 1");
+  FGT_REQUIRE(nt >= 0, FGT_ERR_ARG, "nt must be >= 0");
+  FGT_REQUIRE(iperiod == 0 || iperiod == 1, FGT_ERR_ARG, "iperiod must be 0 or 1");
+  FGT_REQUIRE(sources && bs0 && cen0, FGT_ERR_ARG, "null sources/bs0/cen0");
+  FGT_REQUIRE(!(nt > 0 && !targ), FGT_ERR_ARG, "null targets");
+  FGT_REQUIRE(!(iperiod == 1 && !(*bs0 > 0)), FGT_ERR_ARG, "periodic bs0 must be positive");
+  if (fault_requested("launch") || fault_requested("alloc") || fault_requested("queue"))
+    throw Error{FGT_ERR_INJECTED, "fault injected by FGT_FAULT"};
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    (void)cudaGetLastError();
+    fgt_set_error_message("no CUDA device", __FILE__, __LINE__);
+    throw Error{FGT_ERR_NODEVICE, "no CUDA device"};
+  }
+  int dev = o.device;
+  if (dev < 0) FGT_CUDA(cudaGetDevice(&dev));
+  FGT_CUDA(cudaSetDevice(dev));
+  configure_pool(dev);
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : library_stream(dev);
+  fgt_plan* pl = new fgt_plan();
+  pl->device = dev;
+  pl->o = o;
+  pl->o.stats = nullptr;
+  pl->o.timing = 0;
+  pl->prec = o.precision == FGT_PREC_AUTO
+                 ? ((eps >= 1e-6 * (1 - 1e-9)) ? FGT_PREC_MIXED : FGT_PREC_FP64)
+                 : o.precision;
+  pl->arena = new Arena();
+  try {
+    ArenaOverride ov(pl->arena);
+    Call c = {};
+    c.nd = nd; c.dim = dim; c.iperiod = iperiod; c.ns = ns; c.nt = nt;
+    c.delta = delta; c.eps = eps;
+    DBuf<double> d_src, d_trg;
+    if (o.device_ptrs) {
+      c.src = sources;
+      c.trg = nt > 0 ? targ : sources;
+    } else {
+      d_src.alloc((size_t)ns * dim, s);
+      FGT_CUDA(cudaMemcpyAsync(d_src.get(), sources, sizeof(double) * ns * dim,
+                               cudaMemcpyHostToDevice, s));
+      c.src = d_src;
+      c.trg = c.src;
+      if (nt > 0) {
+        d_trg.alloc((size_t)nt * dim, s);
+        FGT_CUDA(cudaMemcpyAsync(d_trg.get(), targ, sizeof(double) * nt * dim,
+                                 cudaMemcpyHostToDevice, s));
+        c.trg = d_trg;
+      }
+    }
+    Timer tm(false, s);
+    setup_geometry(pl->u, c, bs0, cen0, o, s, tm);
+    FGT_CUDA(cudaStreamSynchronize(s));
+  } catch (...) {
+    cudaStreamSynchronize(s);
+    pl->arena->release_all();
+    delete pl->arena;
+    delete pl;
+    throw;
+  }
+  return pl;
+}
+
+int plan_execute_impl(fgt_plan* pl, int ifcharge, const double* charge, int ifdipole,
+                      const double* rnormal, const double* dipstr, int ifpgh, double* pot,
+                      double* grad, double* hess, int ifpghtarg, double* pottarg,
+                      double* gradtarg, double* hesstarg) {
+  FGT_REQUIRE(pl, FGT_ERR_ARG, "null plan");
+  const Setup& u = pl->u;
+  const int nd = u.nd, dim = u.dim, ns = u.ns, nt = u.nt, nhess = dim * (dim + 1) / 2;
+  FGT_REQUIRE(ifcharge == 1 || ifdipole == 1, FGT_ERR_ARG, "need charges and/or dipoles");
+  FGT_REQUIRE(ifpgh >= 0 && ifpgh <= 3 && ifpghtarg >= 0 && ifpghtarg <= 3, FGT_ERR_ARG,
+              "ifpgh/ifpghtarg must lie in 0..3");
+  FGT_REQUIRE(!(ifcharge == 1 && !charge), FGT_ERR_ARG, "null charge");
+  FGT_REQUIRE(!(ifdipole == 1 && (!dipstr || !rnormal)), FGT_ERR_ARG, "null dipole arrays");
+  FGT_REQUIRE(!(ifpgh >= 1 && !pot) && !(ifpgh >= 2 && !grad) && !(ifpgh >= 3 && !hess),
+              FGT_ERR_ARG, "null source output");
+  const int pght = nt > 0 ? ifpghtarg : 0;
+  FGT_REQUIRE(!(pght >= 1 && !pottarg) && !(pght >= 2 && !gradtarg) && !(pght >= 3 && !hesstarg),
+              FGT_ERR_ARG, "null target output");
+  if (fault_requested("launch") || fault_requested("alloc") || fault_requested("queue"))
+    throw Error{FGT_ERR_INJECTED, "fault injected by FGT_FAULT"};
+  const fgt_opts& o = pl->o;
+  FGT_CUDA(cudaSetDevice(pl->device));
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : library_stream(pl->device);
+  ArenaScope arena_scope(s);
+  Call c = {};
+  c.nd = nd; c.dim = dim; c.iperiod = u.iperiod; c.ns = ns; c.nt = nt;
+  c.ifcharge = ifcharge == 1; c.ifdipole = ifdipole == 1;
+  c.ifpgh = ifpgh; c.ifpghtarg = pght;
+  c.delta = u.delta; c.eps = u.eps;
+  DBuf<double> d_q, d_rn, d_ds, d_pot, d_grad, d_hess, d_pt, d_gt, d_ht;
+  auto h2d = [&](DBuf<double>& b, const double* h, size_t n) -> const double* {
+    if (o.device_ptrs) return h;
+    b.alloc(n, s);
+    FGT_CUDA(cudaMemcpyAsync(b.get(), h, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    return b.get();
+  };
+  auto dout = [&](DBuf<double>& b, double* h, size_t n) -> double* {
+    if (o.device_ptrs) return h;
+    b.alloc(n, s);
+    return b.get();
+  };
+  c.q = c.ifcharge ? h2d(d_q, charge, (size_t)ns * nd) : nullptr;
+  c.rn = c.ifdipole ? h2d(d_rn, rnormal, (size_t)ns * dim) : nullptr;
+  c.ds = c.ifdipole ? h2d(d_ds, dipstr, (size_t)ns * nd) : nullptr;
+  c.pot = ifpgh >= 1 ? dout(d_pot, pot, (size_t)ns * nd) : nullptr;
+  c.grad = ifpgh >= 2 ? dout(d_grad, grad, (size_t)ns * nd * dim) : nullptr;
+  c.hess = ifpgh >= 3 ? dout(d_hess, hess, (size_t)ns * nd * nhess) : nullptr;
+  c.pott = pght >= 1 ? dout(d_pt, pottarg, (size_t)nt * nd) : nullptr;
+  c.gradt = pght >= 2 ? dout(d_gt, gradtarg, (size_t)nt * nd * dim) : nullptr;
+  c.hesst = pght >= 3 ? dout(d_ht, hesstarg, (size_t)nt * nd * nhess) : nullptr;
+  Timer tm(false, s);
+  if (pl->prec == FGT_PREC_FP64) execute<double>(u, c, o, nullptr, s, tm);
+  else execute<float>(u, c, o, nullptr, s, tm);
+  if (!o.device_ptrs) {
+    auto d2h = [&](double* h, const DBuf<double>& b, size_t n) {
+      if (h && b.p) FGT_CUDA(cudaMemcpyAsync(h, b.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    };
+    if (ifpgh >= 1) d2h(pot, d_pot, (size_t)ns * nd);
+    if (ifpgh >= 2) d2h(grad, d_grad, (size_t)ns * nd * dim);
+    if (ifpgh >= 3) d2h(hess, d_hess, (size_t)ns * nd * nhess);
+    if (pght >= 1) d2h(pottarg, d_pt, (size_t)nt * nd);
+    if (pght >= 2) d2h(gradtarg, d_gt, (size_t)nt * nd * dim);
+    if (pght >= 3) d2h(hesstarg, d_ht, (size_t)nt * nd * nhess);
+  }
+  FGT_CUDA(cudaStreamSynchronize(s));
+  return FGT_OK;
+}
+
+}  // namespace
+}  // namespace fgt
+
 extern "C" {
 
 void fgt_opts_default(fgt_opts* o) {
@@ -523,6 +737,56 @@ void pfgt_(const int* nd, const int* dim, const double* delta, const double* eps
     if (*ifpghtarg >= 2) fill(gradtarg, (long long)*nt * n * d);
     if (*ifpghtarg >= 3) fill(hesstarg, (long long)*nt * n * nh);
   }
+}
+
+fgt_plan* fgt_plan_create(const fgt_opts* opts, int nd, int dim, double delta, double eps,
+                          int iperiod, double* bs0, double* cen0, int ns, const double* sources,
+                          int nt, const double* targ, int* status) {
+  fgt_plan* pl = nullptr;
+  int st = FGT_OK;
+  try {
+    pl = fgt::plan_create_impl(opts, nd, dim, delta, eps, iperiod, bs0, cen0, ns, sources, nt,
+                               targ);
+  } catch (const fgt::Error& e) {
+    st = e.code;
+  } catch (...) {
+    fgt_set_error_message("unexpected host exception", __FILE__, __LINE__);
+    st = FGT_ERR_CUDA;
+  }
+  g_last_status = st;
+  if (status) *status = st;
+  return pl;
+}
+
+int fgt_plan_execute(fgt_plan* plan, int ifcharge, const double* charge, int ifdipole,
+                     const double* rnormal, const double* dipstr, int ifpgh, double* pot,
+                     double* grad, double* hess, int ifpghtarg, double* pottarg,
+                     double* gradtarg, double* hesstarg) {
+  int st;
+  try {
+    st = fgt::plan_execute_impl(plan, ifcharge, charge, ifdipole, rnormal, dipstr, ifpgh, pot,
+                                grad, hess, ifpghtarg, pottarg, gradtarg, hesstarg);
+  } catch (const fgt::Error& e) {
+    st = e.code;
+  } catch (...) {
+    fgt_set_error_message("unexpected host exception", __FILE__, __LINE__);
+    st = FGT_ERR_CUDA;
+  }
+  g_last_status = st;
+  return st;
+}
+
+void fgt_plan_destroy(fgt_plan* plan) {
+  if (!plan) return;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(plan->device);
+  if (plan->arena) {
+    plan->arena->release_all();  // cudaFree waits for the device work using it
+    delete plan->arena;
+  }
+  delete plan;
+  cudaSetDevice(cur);
 }
 
 int fgt_last_status(void) { return g_last_status; }

@@ -51,7 +51,13 @@ void Arena::release_all() {
   used = high = 0;
 }
 
+static thread_local Arena* t_arena_override = nullptr;
+
+ArenaOverride::ArenaOverride(Arena* a) : prev(t_arena_override) { t_arena_override = a; }
+ArenaOverride::~ArenaOverride() { t_arena_override = prev; }
+
 Arena* thread_arena() {
+  if (t_arena_override) return t_arena_override;
   static thread_local std::map<int, Arena*> arenas;
   int dev = 0;
   cudaGetDevice(&dev);

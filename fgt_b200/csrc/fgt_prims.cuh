@@ -22,8 +22,16 @@ struct Arena {
   void reset(cudaStream_t s);  // call end: all allocations are dead
   void release_all();
 };
-// Arena of the calling host thread on the current device (created lazily).
+// Arena of the calling host thread on the current device (created lazily),
+// or the arena installed by an ArenaOverride on this thread.
 Arena* thread_arena();
+// RAII: while alive, this thread's device buffers come from `a` (a plan's
+// own arena, which outlives the call).
+struct ArenaOverride {
+  Arena* prev;
+  explicit ArenaOverride(Arena* a);
+  ~ArenaOverride();
+};
 // RAII scope of one library call: resets the arena on exit.
 struct ArenaScope {
   Arena* a;

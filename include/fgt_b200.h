@@ -133,6 +133,37 @@ typedef struct fgt_instance {
 int fgt_pfgt_batch(const fgt_opts *opts, int ninst, fgt_instance *inst, int nworkers);
 
 /*
+ * Reusable plan: the point-dependent part of pfgt kept on the device for
+ * repeated calls on the same sources and targets with new strengths.  The
+ * reference repeats all of it on every call: scalar set-up and tree
+ * (src/pfgt/pfgt.f:110-321, src/common/pts_tree_nd.f:35-1256), lists
+ * (src/common/tree_routs_nd.f:1063-1555) and the sort of the points
+ * (src/common/fmmcommon2d.f:3-27).
+ *
+ * fgt_plan_create takes the geometry arguments of pfgt (bs0/cen0 written in
+ * free space, read when periodic) and the options (precision, device
+ * pointers, device, stream, ndiv, small_eval, spread_width are kept; stats
+ * and timing are ignored); *status receives FGT_OK or an FGT_ERR_* code and
+ * NULL is returned on failure.  fgt_plan_execute takes the strength and
+ * output arguments of pfgt (same layouts; host or device pointers as at
+ * creation) and gives the results of fgt_pfgt_c on the plan's points.  One
+ * plan may be executed from several host threads at once (each thread runs
+ * on its own stream and workspace unless the plan was given a stream).
+ * fgt_plan_destroy releases the plan's device memory.
+ */
+typedef struct fgt_plan fgt_plan;
+fgt_plan *fgt_plan_create(const fgt_opts *opts, int nd, int dim, double delta,
+                          double eps, int iperiod, double *bs0, double *cen0,
+                          int ns, const double *sources, int nt,
+                          const double *targ, int *status);
+int fgt_plan_execute(fgt_plan *plan, int ifcharge, const double *charge,
+                     int ifdipole, const double *rnormal, const double *dipstr,
+                     int ifpgh, double *pot, double *grad, double *hess,
+                     int ifpghtarg, double *pottarg, double *gradtarg,
+                     double *hesstarg);
+void fgt_plan_destroy(fgt_plan *plan);
+
+/*
  * gfortran-mangled drop-in for `call pfgt(...)` (src/pfgt/pfgt.f:6-10): all
  * 24 arguments by reference, no hidden string lengths.  The reference has no
  * error argument; on failure the requested outputs are NaN-filled and the
