@@ -80,6 +80,76 @@ __device__ __forceinline__ void pass_inplace(T* B, int nl, int nb, int SA, int S
   const int t = threadIdx.x, lg = t / nkg, kg = t - lg * nkg;
   const bool act_t = lg < ngroups;
   const int lpr = ngroups * LG;
+  if constexpr (std::is_same<T, float>::value) {
+    // FP32: complex accumulators as FP32x2 pairs (re, im); a complex MAC is
+    // two packed FMAs, (re, im) += (xr, xr)(tr, ti) + (xi, xi)(-ti, tr); the
+    // real-output pass accumulates (xr tr, -xi ti) and adds the halves.
+    for (int r0 = 0; r0 < nl; r0 += lpr) {
+      float2 acc[LG][KG];
+      int base[LG];
+      bool lact[LG];
+#pragma unroll
+      for (int g = 0; g < LG; g++) {
+        const int line = r0 + lg * LG + g;
+        lact[g] = act_t && line < nl;
+        base[g] = lact[g] ? (line / nb) * SA + (line % nb) * SB : 0;
+#pragma unroll
+        for (int j = 0; j < KG; j++) acc[g][j] = make_float2(0.f, 0.f);
+      }
+      if (act_t) {
+        for (int l = 0; l < nin; l++) {
+          float2 t1[KG], t2[KG];
+#pragma unroll
+          for (int j = 0; j < KG; j++) {
+            const int k = kg + j * nkg;  // interleaved: neighbouring lanes, neighbouring modes
+            const bool ok = k < nout;
+            const float tr = ok ? tw[2 * (l * nout + k)] : 0.f;
+            const float ti = ok ? tw[2 * (l * nout + k) + 1] : 0.f;
+            t1[j] = MODE == 2 ? make_float2(tr, -ti) : make_float2(tr, ti);
+            t2[j] = make_float2(-ti, tr);
+          }
+#pragma unroll
+          for (int g = 0; g < LG; g++) {
+            if (!lact[g]) continue;
+            if (MODE == 0) {
+              const float gv = B[base[g] + l * ein];
+              const float2 gg = make_float2(gv, gv);
+#pragma unroll
+              for (int j = 0; j < KG; j++) acc[g][j] = __ffma2_rn(gg, t1[j], acc[g][j]);
+            } else if (MODE == 1) {
+              const float xr = B[base[g] + l * ein], xi = B[base[g] + l * ein + 1];
+              const float2 rr = make_float2(xr, xr), ii = make_float2(xi, xi);
+#pragma unroll
+              for (int j = 0; j < KG; j++)
+                acc[g][j] = __ffma2_rn(ii, t2[j], __ffma2_rn(rr, t1[j], acc[g][j]));
+            } else {
+              const float2 x = make_float2(B[base[g] + l * ein], B[base[g] + l * ein + 1]);
+#pragma unroll
+              for (int j = 0; j < KG; j++) acc[g][j] = __ffma2_rn(x, t1[j], acc[g][j]);
+            }
+          }
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int g = 0; g < LG; g++) {
+        if (!lact[g]) continue;
+#pragma unroll
+        for (int j = 0; j < KG; j++) {
+          const int k = kg + j * nkg;
+          if (k >= nout) break;
+          if (MODE == 2) {
+            B[base[g] + k * eout] = acc[g][j].x + acc[g][j].y;
+          } else {
+            B[base[g] + k * eout] = acc[g][j].x;
+            B[base[g] + k * eout + 1] = acc[g][j].y;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    return;
+  }
   for (int r0 = 0; r0 < nl; r0 += lpr) {
     T re[LG][KG], im[LG][KG];
     int base[LG];
