@@ -279,7 +279,8 @@ def main():
         o.device = local
         o.stream = C.c_void_p(stream.cuda_stream)
         o.timing = 1 if timing else 0
-        o.stats = C.pointer(st)
+        # statistics (device read-backs) only in the untimed phase pass
+        o.stats = C.pointer(st) if timing else None
         return o
 
     od = opts(1, False)  # timed steps: no per-phase events

@@ -347,8 +347,8 @@ void execute(const Setup& u, const Call& c, const fgt_opts& o, fgt_stats* st, cu
   g.center = t.center;
   g.level = t.level;
   double pairs = 0;
-  launches += direct_near_field<T>(g, L, src, et, &pairs, s);
-  launches += direct_near_field<T>(g, L, src, es, &pairs, s);
+  launches += direct_near_field<T>(g, L, src, et, st ? &pairs : nullptr, s);
+  launches += direct_near_field<T>(g, L, src, es, st ? &pairs : nullptr, s);
   tm.mark(7);
   // --- back to input order
   if (c.ifpgh >= 1) {

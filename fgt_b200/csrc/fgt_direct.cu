@@ -15,7 +15,8 @@ constexpr int DW = 4;  // warps per block
 
 template <typename T>
 struct DArgs {
-  int n_items, nd, d0, ne, ns, iperiod0;
+  int n_items, nd, d0, ne, ns, iperiod0;  // n_items: upper bound
+  const int* n_items_dev;                  // item count on the device
   T dinv, dmax, rfac;  // 1/delta, cut-off, 2/delta
   double bs0;
   const int *item_box, *item_lo;
@@ -75,7 +76,8 @@ __global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
   __shared__ T sn[DW][DIP ? DIM : 1][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ndc = min(NDC, a.nd - a.d0);
-  for (int it = blockIdx.x * DW + warp; it < a.n_items; it += gridDim.x * DW) {
+  const int n_items = *a.n_items_dev;
+  for (int it = blockIdx.x * DW + warp; it < n_items; it += gridDim.x * DW) {
     const int tb = a.item_box[it];
     const int p = a.item_lo[it] + lane;
     const bool act = p < a.e_hi[tb];
@@ -247,7 +249,8 @@ __global__ void __launch_bounds__(DW * 32) k_direct32(DArgs<float> a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ndc = min(NDC, a.nd - a.d0);
   const float ce = a.dinv * 1.4426950408889634f;  // exp(-rr/delta) = 2^(-rr*ce)
-  for (int it = blockIdx.x * DW + warp; it < a.n_items; it += gridDim.x * DW) {
+  const int n_items = *a.n_items_dev;
+  for (int it = blockIdx.x * DW + warp; it < n_items; it += gridDim.x * DW) {
     const int tb = a.item_box[it];
     const int p = a.item_lo[it] + lane;
     const bool act = p < a.e_hi[tb];
@@ -426,7 +429,8 @@ __global__ void __launch_bounds__(DW * 32) k_direct32x2(DArgs<float> a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const float ce = a.dinv * 1.4426950408889634f;  // exp(-rr/delta) = 2^(-rr*ce)
   const float2 nce = make_float2(-ce, -ce), nrf = make_float2(-a.rfac, -a.rfac);
-  for (int it = blockIdx.x * DW + warp; it < a.n_items; it += gridDim.x * DW) {
+  const int n_items = *a.n_items_dev;
+  for (int it = blockIdx.x * DW + warp; it < n_items; it += gridDim.x * DW) {
     const int tb = a.item_box[it];
     const int pA = a.item_lo[it] + lane, pB = pA + 32;
     const int ehi = a.e_hi[tb];
@@ -606,21 +610,22 @@ int direct_near_field(const DirectGeom& g, const Lists& L, const SourceSet<T>& s
                                                    pairs ? dpairs.get() : nullptr);
   FGT_LAUNCH_CHECK();
   exclusive_scan_i32(cnt, pos, nb, tot, s);
-  int n_items = fetch_int(tot, s);
-  if (pairs) {
+  if (pairs) {  // statistics only: the one read-back of this function
     double h = 0;
     FGT_CUDA(cudaMemcpyAsync(&h, dpairs.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
     FGT_CUDA(cudaStreamSynchronize(s));
     *pairs += h;
   }
   launches += 2;
-  if (n_items == 0) return launches;
+  // the item count stays on the device: sum_b ceil(ne_b / tpi) <= ne / tpi + nboxes
+  const int n_items = (int)std::min<long long>((long long)e.n / tpi + nb + 1, INT32_MAX);
   DBuf<int> ibox(n_items, s), ilo(n_items, s);
   k_items_fill<<<grid_for(nb, 128), 128, 0, s>>>(nb, tpi, cnt, pos, e.lo, ibox, ilo);
   FGT_LAUNCH_CHECK();
   launches++;
   DArgs<T> a;
   a.n_items = n_items;
+  a.n_items_dev = tot;
   a.nd = g.nd;
   a.ne = e.n;
   a.ns = src.n;

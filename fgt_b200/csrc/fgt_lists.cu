@@ -238,6 +238,14 @@ TV make_tv(const Tree& t, int npwlevel, int iperiod0, int nlevend) {
 
 }  // namespace
 
+namespace {
+__global__ void k_eval_self(int n_eval, const int* __restrict__ eval_box,
+                            const int* __restrict__ fslot, int lo, int* __restrict__ eval_self) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_eval; e += gridDim.x * blockDim.x)
+    eval_self[e] = fslot[eval_box[e] - lo];
+}
+}  // namespace
+
 void build_lists(const Tree& t, int npwlevel, int iperiod0, int nlevend, bool do_pw, Lists& L,
                  cudaStream_t s) {
   TV tv = make_tv(t, npwlevel, iperiod0, nlevend);
@@ -272,16 +280,10 @@ void build_lists(const Tree& t, int npwlevel, int iperiod0, int nlevend, bool do
   k_compact_idx<<<grid_for(n, 256), 256, 0, s>>>(fe, pe, n, lo, L.eval_box, nullptr);
   FGT_LAUNCH_CHECK();
   // eval_self[e] = form slot of eval box e
-  {
-    std::vector<int> hs(n), he(std::max(L.n_eval, 1)), hself(std::max(L.n_eval, 1));
-    FGT_CUDA(cudaMemcpyAsync(hs.data(), fslot.get(), sizeof(int) * n, cudaMemcpyDeviceToHost, s));
-    FGT_CUDA(cudaMemcpyAsync(he.data(), L.eval_box.get(), sizeof(int) * L.n_eval,
-                             cudaMemcpyDeviceToHost, s));
-    FGT_CUDA(cudaStreamSynchronize(s));
-    for (int e = 0; e < L.n_eval; e++) hself[e] = hs[he[e] - lo];
-    FGT_CUDA(cudaMemcpyAsync(L.eval_self.get(), hself.data(), sizeof(int) * L.n_eval,
-                             cudaMemcpyHostToDevice, s));
-    FGT_CUDA(cudaStreamSynchronize(s));
+  if (L.n_eval > 0) {
+    k_eval_self<<<grid_for(L.n_eval, 256), 256, 0, s>>>(L.n_eval, L.eval_box, fslot, lo,
+                                                         L.eval_self);
+    FGT_LAUNCH_CHECK();
   }
   L.trans_ptr.alloc(L.n_eval + 1, s);
   {

@@ -567,7 +567,7 @@ int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>
   }
   PWArgs<T> a;
   DevTables<T> tb;
-  make_args<T>(P, a, tb, s, false);
+  make_args<T>(P, a, tb, s, false, 0);
   D.mp.alloc((size_t)L.n_form * P.nd * 2 * P.nexp, s);
   FormIO io;
   io.n_form = L.n_form;
@@ -611,8 +611,10 @@ int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, PWWork* work, 
   int nsh = P.dim == 1 ? 3 : (P.dim == 2 ? 9 : 27);
   D.wtab.alloc((size_t)nsh * 2 * P.nexp, s);
   DBuf<double> ts64(P.ts.size(), s);
-  FGT_CUDA(cudaMemcpyAsync(ts64.get(), P.ts.data(), sizeof(double) * P.ts.size(),
-                           cudaMemcpyHostToDevice, s));
+  double* hts = static_cast<double*>(pinned_stage(2, sizeof(double) * P.ts.size()));
+  std::copy(P.ts.begin(), P.ts.end(), hts);
+  FGT_CUDA(cudaMemcpyAsync(ts64.get(), hts, sizeof(double) * P.ts.size(), cudaMemcpyHostToDevice,
+                           s));
   k_wtab<T><<<grid_for((long long)nsh * P.nexp, 256), 256, 0, s>>>(P.dim, P.K, P.nexp, ts64,
                                                                    P.xmin, D.wtab);
   FGT_LAUNCH_CHECK();
@@ -630,7 +632,6 @@ int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, PWWork* work, 
                                         D.wtab, D.loc.get() + (size_t)e0 * P.nd * 2 * P.nexp);
     FGT_LAUNCH_CHECK();
   }
-  FGT_CUDA(cudaStreamSynchronize(s));  // ts64 lifetime
   return 2;
 }
 

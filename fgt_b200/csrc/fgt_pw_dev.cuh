@@ -702,14 +702,31 @@ int supported_w(int w) {
 
 template <typename T>
 struct DevTables {
-  DBuf<T> twf, twh, tif, tih, facf, faci, ts;
+  DBuf<T> all;  // twf, twh, tif, tih, facf, faci, ts back to back
 };
 
-// Device arguments for grid parameters P; the innermost buffer stride is
-// padded to W (mod 32) words for FP32 so the warp-per-point stencils are
-// bank-conflict free.
+// Pinned host staging of small host-computed tables, per host thread and
+// slot (0: form tables, 1: evaluation tables, 2: translation nodes).  The
+// tables go to the device with one asynchronous copy (a pageable source would
+// make the copy wait for the stream); a slot is rewritten only by a later
+// call, after that call's final stream synchronisation.
+inline void* pinned_stage(int slot, size_t bytes) {
+  static thread_local void* buf[3] = {nullptr, nullptr, nullptr};
+  static thread_local size_t cap[3] = {0, 0, 0};
+  if (cap[slot] < bytes) {
+    if (buf[slot]) cudaFreeHost(buf[slot]);
+    buf[slot] = nullptr;
+    cap[slot] = 0;
+    const size_t want = std::max(bytes, (size_t)1 << 20);
+    FGT_CUDA(cudaHostAlloc(&buf[slot], want, cudaHostAllocDefault));
+    cap[slot] = want;
+  }
+  return buf[slot];
+}
+
 template <typename T>
-void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s, bool pad) {
+void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s, bool pad,
+               int slot) {
   Geo& g = a.g;
   g.dim = P.dim;
   g.K = P.K;
@@ -748,7 +765,11 @@ void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s
   a.beta = (T)P.beta;
   a.dscale = (T)(a.inv_dx_d * a.scale_d / a.hwdx_d);
   a.inv_sqd0 = (T)(1.0 / P.sqd0);
-  std::vector<T> twf(2 * G * NF), twh(2 * G * NH), tif(2 * NF * G), tih(2 * NH * G);
+  const size_t ntwf = 2 * (size_t)G * NF, ntwh = 2 * (size_t)G * NH, ntif = 2 * (size_t)NF * G,
+               ntih = 2 * (size_t)NH * G, total = ntwf + ntwh + ntif + ntih + 3 * (size_t)NF;
+  T* h = static_cast<T*>(pinned_stage(slot, sizeof(T) * total));
+  T *twf = h, *twh = twf + ntwf, *tif = twh + ntwh, *tih = tif + ntif;
+  T *facf = tih + ntih, *faci = facf + NF, *ts = faci + NF;
   for (int l = 0; l < G; l++) {
     double xl = (double)(P.l0 + l) * P.dx;
     for (int k = -K; k <= K; k++) {
@@ -766,31 +787,21 @@ void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s
       }
     }
   }
-  std::vector<T> facf(NF), faci(NF), ts(NF);
   for (int k = 0; k < NF; k++) {
     facf[k] = (T)(P.dx * P.wsym[k] / P.phihat[k]);
     faci[k] = (T)(P.dx / P.phihat[k]);
     ts[k] = (T)P.ts[k];
   }
-  auto up = [&](DBuf<T>& b, const std::vector<T>& h) {
-    b.alloc(h.size(), s);
-    FGT_CUDA(cudaMemcpyAsync(b.get(), h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
-  };
-  up(tb.twf, twf);
-  up(tb.twh, twh);
-  up(tb.tif, tif);
-  up(tb.tih, tih);
-  up(tb.facf, facf);
-  up(tb.faci, faci);
-  up(tb.ts, ts);
-  FGT_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
-  a.twf = tb.twf;
-  a.twh = tb.twh;
-  a.tif = tb.tif;
-  a.tih = tb.tih;
-  a.facf = tb.facf;
-  a.faci = tb.faci;
-  a.ts = tb.ts;
+  tb.all.alloc(total, s);
+  FGT_CUDA(cudaMemcpyAsync(tb.all.get(), h, sizeof(T) * total, cudaMemcpyHostToDevice, s));
+  T* d = tb.all.get();
+  a.twf = d;
+  a.twh = d + ntwf;
+  a.tif = a.twh + ntwh;
+  a.tih = a.tif + ntif;
+  a.facf = a.tih + ntih;
+  a.faci = a.facf + NF;
+  a.ts = a.faci + NF;
   a.gscratch = nullptr;
 }
 

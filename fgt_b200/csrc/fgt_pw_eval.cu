@@ -17,7 +17,8 @@ struct EvalPtrs {
   const T* loc;      // [n_eval][nd][nexp]
   const int* boxes;  // eval slots handled by this launch
   const int* eval_box;
-  int nbox;
+  int nbox;             // upper bound (grid sizing)
+  const int* nbox_dev;  // actual count on the device, or null: nbox
   // two evaluation sets (sources, targets)
   const double* off[2];
   const int* lo[2];
@@ -138,7 +139,8 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<
   load_tw(tif, a.tif, 2 * NF * G);
   load_tw(tih, a.tih, 2 * NH * G);
   __syncthreads();
-  for (int bi = blockIdx.x; bi < p.nbox; bi += gridDim.x) {
+  const int nbox = p.nbox_dev ? *p.nbox_dev : p.nbox;
+  for (int bi = blockIdx.x; bi < nbox; bi += gridDim.x) {
     const int e = p.boxes[bi];
     const int box = p.eval_box[e];
     for (int id = 0; id < p.nd; id++) {
@@ -211,7 +213,8 @@ __global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal(PWArgs<T> a, EvalP
   double* red = reinterpret_cast<double*>(smem_raw);        // [NW][32][NCM]
   T* E = reinterpret_cast<T*>(red + (size_t)NW * 32 * NCM);  // [NE][pmax] complex
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int bi = blockIdx.x; bi < p.nbox; bi += gridDim.x) {
+  const int nbox = p.nbox_dev ? *p.nbox_dev : p.nbox;
+  for (int bi = blockIdx.x; bi < nbox; bi += gridDim.x) {
     const int e = p.boxes[bi];
     const int box = p.eval_box[e];
     const int n0 = p.n[0] > 0 && p.ncomp[0] > 0 ? p.hi[0][box] - p.lo[0][box] : 0;
@@ -347,7 +350,12 @@ __global__ void k_eval_split(int n_eval, const int* __restrict__ eval_box, const
   }
 }
 __global__ void k_split_fill(int n, const int* __restrict__ f, const int* __restrict__ pos,
-                             int* __restrict__ big_list, int* __restrict__ small_list) {
+                             int* __restrict__ big_list, int* __restrict__ small_list,
+                             const int* __restrict__ nbig, int* __restrict__ counts) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counts[0] = *nbig;
+    counts[1] = n - *nbig;
+  }
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
     if (f[e]) big_list[pos[e]] = e;
     else small_list[e - pos[e]] = e;
@@ -446,7 +454,7 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   if (deriv) pw_grid(Pe, wgrad, true);
   PWArgs<T> a;
   DevTables<T> tb;
-  make_args<T>(Pe, a, tb, s, false);
+  make_args<T>(Pe, a, tb, s, false, 1);
   int launches = 0;
   // boxes with at most thr evaluation points use the modal sums; thr is
   // capped by the modal kernel's shared memory (per point: FP64 partials of
@@ -464,14 +472,16 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
       u1 ? e1.hi : nullptr, thr, big, cnt);
   FGT_LAUNCH_CHECK();
   exclusive_scan_i32(big, pos, L.n_eval, tot, s);
-  int nbig = fetch_int(tot, s);
-  DBuf<int> lbig(std::max(nbig, 1), s), lsmall(std::max(L.n_eval - nbig, 1), s);
-  k_split_fill<<<grid_for(L.n_eval, 256), 256, 0, s>>>(L.n_eval, big, pos, lbig, lsmall);
+  // both lists sized for all eval boxes; the counts stay on the device
+  DBuf<int> lbig(L.n_eval, s), lsmall(L.n_eval, s), counts(2, s);
+  k_split_fill<<<grid_for(L.n_eval, 256), 256, 0, s>>>(L.n_eval, big, pos, lbig, lsmall, tot,
+                                                        counts);
   FGT_LAUNCH_CHECK();
   launches += 3;
   int nh = P.dim * (P.dim + 1) / 2;
   auto ncomp = [&](int pgh) { return pgh <= 0 ? 0 : 1 + (pgh >= 2 ? P.dim : 0) + (pgh >= 3 ? nh : 0); };
   EvalPtrs<T> ep;
+  ep.nbox_dev = nullptr;
   ep.loc = D.loc;
   ep.eval_box = L.eval_box;
   ep.nd = P.nd;
@@ -487,17 +497,17 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   }
   ep.ncomp_max = std::max(ep.ncomp[0], ep.ncomp[1]);
   DBuf<T> gs;
-  if (nbig > 0) {
+  {
     ep.boxes = lbig;
-    ep.nbox = nbig;
+    ep.nbox = L.n_eval;
+    ep.nbox_dev = counts.get();
     launches += eval_dim<T>(P.dim, Pe.w, a, ep, deriv, gs, s);
-    if (work) work->n_nufft += nbig;
   }
-  int nsmall = L.n_eval - nbig;
-  if (nsmall > 0) {
+  {
     ep.boxes = lsmall;
-    ep.nbox = nsmall;
-    int grid = std::max(1, std::min(nsmall, kSMs * 8));
+    ep.nbox = L.n_eval;
+    ep.nbox_dev = counts.get() + 1;
+    int grid = std::max(1, std::min(L.n_eval, kSMs * 8));
     size_t sm = modal_fix + modal_pt * (size_t)std::max(thr, 1);
     if (P.dim == 1) {
       set_smem(k_eval_modal<T, 1>, sm);
@@ -514,8 +524,12 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   }
   if (work) {
     unsigned long long h[2] = {0, 0};
+    int hc[2] = {0, 0};
     FGT_CUDA(cudaMemcpyAsync(h, cnt.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    FGT_CUDA(cudaMemcpyAsync(hc, counts.get(), sizeof(hc), cudaMemcpyDeviceToHost, s));
     FGT_CUDA(cudaStreamSynchronize(s));
+    const int nbig = hc[0];
+    work->n_nufft += nbig;
     const double wd = pow((double)Pe.w, P.dim);
     const double grids = mode == 2 ? ep.ncomp_max : 1;
     // derivative mode: value and derivative sums along the last dimension
@@ -527,7 +541,6 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
     work->w_eval = Pe.w;
     work->G_eval = Pe.G;
   }
-  FGT_CUDA(cudaStreamSynchronize(s));  // tables lifetime
   return launches;
 }
 

@@ -286,6 +286,12 @@ void tree_setup_scalars(int dim, double delta, double eps, int iperiod, const do
   *bs0 = ldexp(1.0, *levcut) * dc;
 }
 
+namespace {
+__global__ void k_fill_int(int* __restrict__ a, int n, int v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
+}
+}  // namespace
+
 void tree_build(Tree& t, int dim, int iperiod, int npwlevel, int ndiv, double bs0,
                 const double* cen0, const double* d_src, int ns, const double* d_trg, int nt,
                 cudaStream_t s) {
@@ -398,13 +404,12 @@ void tree_build(Tree& t, int dim, int iperiod, int npwlevel, int ndiv, double bs
   t.parent.alloc(nboxes, s);
   t.child0.alloc(nboxes, s);
   t.center.alloc((size_t)nboxes * dim, s);
-  {
-    std::vector<int> hlev(nboxes);
-    for (int l = 0; l <= nlevels; l++)
-      for (int i = t.lev_start[l]; i < t.lev_start[l + 1]; i++) hlev[i] = l;
-    FGT_CUDA(cudaMemcpyAsync(t.level.get(), hlev.data(), sizeof(int) * nboxes,
-                             cudaMemcpyHostToDevice, s));
-    FGT_CUDA(cudaStreamSynchronize(s));
+  for (int l = 0; l <= nlevels; l++) {
+    const int n = t.lev_start[l + 1] - t.lev_start[l];
+    if (n > 0) {
+      k_fill_int<<<grid_for(n, 256), 256, 0, s>>>(t.level.get() + t.lev_start[l], n, l);
+      FGT_LAUNCH_CHECK();
+    }
   }
   for (int l = 0; l <= nlevels; l++) {
     FGT_CUDA(cudaMemcpyAsync(t.key.get() + t.lev_start[l], lk[l].get(),
