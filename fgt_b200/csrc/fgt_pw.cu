@@ -3,6 +3,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <utility>
 #include <vector>
 
 #include "fgt_pw_dev.cuh"
@@ -16,6 +17,8 @@ struct FormIO {
   int n_form, ns, nd, ncomp;  // ncomp: charge (1) and/or dipole (dim)
   int has_q, has_dip;
   const int *form_box, *s_lo, *s_hi;
+  const int* order;  // form slots, most sources first
+  int* next;         // work counter (zero at launch)
 };
 
 template <typename T>
@@ -232,7 +235,14 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
   load_tw(twf, a.twf, 2 * G * NF);
   load_tw(twh, a.twh, 2 * G * NH);
   __syncthreads();
-  for (int fb = blockIdx.x; fb < io.n_form; fb += gridDim.x) {
+  // boxes in decreasing source count, each CTA takes the next one
+  __shared__ int s_next;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_next = atomicAdd(io.next, 1);
+    __syncthreads();
+    if (s_next >= io.n_form) break;
+    const int fb = io.order[s_next];
     const int box = io.form_box[fb];
     const int p0 = io.s_lo[box], p1 = io.s_hi[box];
     for (int id = 0; id < io.nd; id++) {
@@ -493,8 +503,14 @@ void pw_grid(PWParams& P, int w, bool exact_w) {
               "plane-wave expansion too long for the spreading kernels");
   // Fourier transform of the kernel, Gauss-Legendre on [-halfw, halfw]
   P.phihat.assign(NF, 0);
-  std::vector<double> xq, wq;
-  legendre(200, xq, wq);
+  // 200-point Gauss-Legendre rule, computed once per process
+  static const std::pair<std::vector<double>, std::vector<double>> gl = [] {
+    std::pair<std::vector<double>, std::vector<double>> r;
+    legendre(200, r.first, r.second);
+    return r;
+  }();
+  const std::vector<double>& xq = gl.first;
+  const std::vector<double>& wq = gl.second;
   for (int k = -K; k <= K; k++) {
     double acc = 0;
     for (size_t i = 0; i < xq.size(); i++) {
@@ -579,6 +595,22 @@ int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>
   io.form_box = L.form_box;
   io.s_lo = src.lo;
   io.s_hi = src.hi;
+  // longest-processing-time order of the form boxes (by source count) and a
+  // work counter: the boxes' costs vary by several times, so a fixed
+  // round-robin assignment leaves CTAs idle at the end
+  DBuf<uint64_t> okey(std::max(L.n_form, 1), s), otmp(std::max(L.n_form, 1), s);
+  DBuf<uint32_t> oval(std::max(L.n_form, 1), s), vtmp(std::max(L.n_form, 1), s);
+  DBuf<int> next(1, s);
+  next.zero();
+  if (L.n_form > 0) {
+    k_lpt_keys<<<grid_for(L.n_form, 256), 256, 0, s>>>(L.n_form, nullptr, L.form_box, nullptr,
+                                                       src.lo, src.hi, nullptr, nullptr, okey,
+                                                       oval);
+    FGT_LAUNCH_CHECK();
+    radix_sort(okey, oval, otmp, vtmp, L.n_form, LPT_BITS, s);
+  }
+  io.order = reinterpret_cast<const int*>(oval.get());
+  io.next = next;
   FormPtrs<T> fp;
   fp.off = src.off;
   fp.q = src.q;

@@ -22,6 +22,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "fgt_prims.cuh"
 #include "fgt_pw.cuh"
 
 namespace fgt {
@@ -686,6 +687,33 @@ __device__ __forceinline__ void order_cells(const PWArgs<T>& a, const double* of
 template <typename T>
 __host__ __device__ constexpr size_t eval_offset(int G, int K) {
   return order_offset<T>(G, K) + sizeof(int) * (NBINS_MAX + 32);
+}
+
+// Keys of a longest-processing-time order: entry i of a box list (list[i]
+// indexes `box`; the identity when list is null) gets key MAXC - cost, with
+// cost = points of the box in one or two evaluation sets, so an ascending
+// sort puts the most expensive boxes first.  Entries at or beyond *count
+// (when count is given) sort after all others.
+constexpr int LPT_BITS = 25;
+__global__ void k_lpt_keys(int n, const int* __restrict__ count, const int* __restrict__ box,
+                           const int* __restrict__ list, const int* __restrict__ lo0,
+                           const int* __restrict__ hi0, const int* __restrict__ lo1,
+                           const int* __restrict__ hi1, uint64_t* __restrict__ keys,
+                           uint32_t* __restrict__ vals) {
+  const int m = count ? *count : n;
+  constexpr uint64_t MAXC = (1ull << (LPT_BITS - 1)) - 1;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int e = list ? list[i] : i;
+    vals[i] = (uint32_t)e;
+    if (i >= m) {
+      keys[i] = 1ull << (LPT_BITS - 1);
+      continue;
+    }
+    const int b = box[e];
+    long long c = (long long)(hi0[b] - lo0[b]) + (lo1 ? (long long)(hi1[b] - lo1[b]) : 0);
+    c = c < 0 ? 0 : (c > (long long)MAXC ? (long long)MAXC : c);
+    keys[i] = MAXC - (uint64_t)c;
+  }
 }
 
 template <typename T>

@@ -19,6 +19,7 @@ struct EvalPtrs {
   const int* eval_box;
   int nbox;             // upper bound (grid sizing)
   const int* nbox_dev;  // actual count on the device, or null: nbox
+  int* next;            // work counter of the grid kernel (zero at launch)
   // two evaluation sets (sources, targets)
   const double* off[2];
   const int* lo[2];
@@ -140,7 +141,14 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<
   load_tw(tih, a.tih, 2 * NH * G);
   __syncthreads();
   const int nbox = p.nbox_dev ? *p.nbox_dev : p.nbox;
-  for (int bi = blockIdx.x; bi < nbox; bi += gridDim.x) {
+  // boxes in decreasing point count, each CTA takes the next one
+  __shared__ int s_next;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_next = atomicAdd(p.next, 1);
+    __syncthreads();
+    const int bi = s_next;
+    if (bi >= nbox) break;
     const int e = p.boxes[bi];
     const int box = p.eval_box[e];
     for (int id = 0; id < p.nd; id++) {
@@ -482,6 +490,7 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   auto ncomp = [&](int pgh) { return pgh <= 0 ? 0 : 1 + (pgh >= 2 ? P.dim : 0) + (pgh >= 3 ? nh : 0); };
   EvalPtrs<T> ep;
   ep.nbox_dev = nullptr;
+  ep.next = nullptr;
   ep.loc = D.loc;
   ep.eval_box = L.eval_box;
   ep.nd = P.nd;
@@ -498,10 +507,22 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   ep.ncomp_max = std::max(ep.ncomp[0], ep.ncomp[1]);
   DBuf<T> gs;
   {
+    // longest-processing-time order of the grid boxes (by point count)
+    DBuf<uint64_t> okey(L.n_eval, s), otmp(L.n_eval, s);
+    DBuf<uint32_t> vtmp(L.n_eval, s);
+    DBuf<int> next(1, s);
+    next.zero();
+    k_lpt_keys<<<grid_for(L.n_eval, 256), 256, 0, s>>>(
+        L.n_eval, counts.get(), L.eval_box, lbig, u0 ? e0.lo : e1.lo, u0 ? e0.hi : e1.hi,
+        (u0 && u1) ? e1.lo : nullptr, (u0 && u1) ? e1.hi : nullptr, okey,
+        reinterpret_cast<uint32_t*>(lbig.get()));
+    FGT_LAUNCH_CHECK();
+    radix_sort(okey, reinterpret_cast<uint32_t*>(lbig.get()), otmp, vtmp, L.n_eval, LPT_BITS, s);
     ep.boxes = lbig;
     ep.nbox = L.n_eval;
     ep.nbox_dev = counts.get();
-    launches += eval_dim<T>(P.dim, Pe.w, a, ep, deriv, gs, s);
+    ep.next = next;
+    launches += 2 + eval_dim<T>(P.dim, Pe.w, a, ep, deriv, gs, s);
   }
   {
     ep.boxes = lsmall;
