@@ -158,11 +158,35 @@ struct Setup {
   Lists L;
   DBuf<double> soff, toff;
   DBuf<uint32_t> inv_s, inv_t;
+  // packed list-1 sources of the FP32 charge path: record count (-1: not
+  // built) and the positions of every list entry's records
+  long long near_total = -1;
+  DBuf<int> near_pos;
   int launches = 0;
 };
 
+// Records of the packed list-1 sources are 64 bytes; above this count (4 GiB)
+// the near field walks the list instead.
+constexpr long long kMaxNearRecords = 1ll << 26;
+
+DirectGeom direct_geom(const Setup& u) {
+  DirectGeom g;
+  g.dim = u.dim;
+  g.nd = u.nd;
+  g.iperiod0 = u.iperiod0;
+  g.nboxes = u.t.nboxes;
+  g.delta = u.delta;
+  g.dmax = log(1.0 / u.eps) * u.delta;
+  g.bs0 = u.t.boxsize[0];
+  g.center = u.t.center;
+  g.level = u.t.level;
+  return g;
+}
+
+// near_lists: build the positions of the packed list-1 sources (FP32, one
+// density; used by executions with charges only and pgh <= 2).
 void setup_geometry(Setup& u, const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
-                    cudaStream_t s, Timer& tm) {
+                    bool near_lists, cudaStream_t s, Timer& tm) {
   const int dim = c.dim;
   u.dim = dim;
   u.nd = c.nd;
@@ -259,11 +283,16 @@ void setup_geometry(Setup& u, const Call& c, double* bs0_io, double* cen0_io, co
     launches++;
   }
   u.npwlevel = npwlevel;
+  u.iperiod0 = iperiod0;
+  if (near_lists && u.L.n_l1 > 0) {
+    u.near_total = near_lists_count(direct_geom(u), u.L, t.src_lo, t.src_hi, t.trg_lo, t.trg_hi,
+                                    u.soff, c.ns, kMaxNearRecords, u.near_pos, s);
+    launches += 2;
+  }
   u.ndiv = ndiv;
   u.nlevels = nlevels;
   u.npw = npw;
   u.pmax = pmax;
-  u.iperiod0 = iperiod0;
   u.periodic_nodes = periodic_nodes;
   u.nlevend = nlevend;
   u.do_pw = do_pw;
@@ -336,19 +365,22 @@ void execute(const Setup& u, const Call& c, const fgt_opts& o, fgt_stats* st, cu
     }
   }
   // --- direct near field (pfgt.f:1082-1136)
-  DirectGeom g;
-  g.dim = dim;
-  g.nd = nd;
-  g.iperiod0 = u.iperiod0;
-  g.nboxes = t.nboxes;
-  g.delta = c.delta;
-  g.dmax = log(1.0 / c.eps) * c.delta;
-  g.bs0 = t.boxsize[0];
-  g.center = t.center;
-  g.level = t.level;
+  const DirectGeom g = direct_geom(u);
   double pairs = 0;
-  launches += direct_near_field<T>(g, L, src, et, st ? &pairs : nullptr, s);
-  launches += direct_near_field<T>(g, L, src, es, st ? &pairs : nullptr, s);
+  NearPacked packed;
+  DBuf<float4> near_rec;
+  if constexpr (sizeof(T) == 4) {
+    if (u.near_total > 0 && nd == 1 && c.ifcharge && !c.ifdipole && c.ifpgh <= 2 &&
+        c.ifpghtarg <= 2) {
+      near_rec.alloc((size_t)u.near_total * 4, s);
+      near_lists_fill(g, L, src, t.trg_lo, t.trg_hi, u.near_pos, near_rec, s);
+      launches++;
+      packed.pos = u.near_pos;
+      packed.rec = near_rec;
+    }
+  }
+  launches += direct_near_field<T>(g, L, src, et, st ? &pairs : nullptr, s, &packed);
+  launches += direct_near_field<T>(g, L, src, es, st ? &pairs : nullptr, s, &packed);
   tm.mark(7);
   // --- back to input order
   if (c.ifpgh >= 1) {
@@ -400,7 +432,10 @@ template <typename T>
 void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o, fgt_stats* st,
               cudaStream_t s, Timer& tm) {
   Setup u;
-  setup_geometry(u, c, bs0_io, cen0_io, o, s, tm);
+  // the packed near-field path: FP32, one density, charges only, pgh <= 2
+  const bool near = sizeof(T) == 4 && c.nd == 1 && c.ifcharge && !c.ifdipole && c.ifpgh <= 2 &&
+                    c.ifpghtarg <= 2;
+  setup_geometry(u, c, bs0_io, cen0_io, o, near, s, tm);
   execute<T>(u, c, o, st, s, tm);
 }
 
@@ -594,7 +629,7 @@ fgt_plan* plan_create_impl(const fgt_opts* opts_in, int nd, int dim, double delt
       }
     }
     Timer tm(false, s);
-    setup_geometry(pl->u, c, bs0, cen0, o, s, tm);
+    setup_geometry(pl->u, c, bs0, cen0, o, pl->prec != FGT_PREC_FP64 && nd == 1, s, tm);
     FGT_CUDA(cudaStreamSynchronize(s));
   } catch (...) {
     cudaStreamSynchronize(s);

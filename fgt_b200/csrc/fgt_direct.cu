@@ -538,6 +538,213 @@ __global__ void __launch_bounds__(DW * 32) k_direct32x2(DArgs<float> a) {
   }
 }
 
+// Packed list-1 sources.  For every target box, the sources of its list-1
+// boxes that can reach the box (minimum distance to the box below the
+// cut-off; the pairs of the others all fail the cut-off test), in list
+// order, each as four float4 of the staging layout of k_direct32x2: FP32
+// hi/lo splits of the FP64 source offset from the target box centre, negated
+// and duplicated, and the charge.  Built once per call and shared by the
+// source and target evaluation sets, so the near-field kernel streams one
+// contiguous array per target box instead of walking the list (dependent
+// loads of box ids, centres, ranges and FP64 offsets per list entry, and
+// source batches shorter than a warp).  COUNT mode writes the kept count of
+// every list entry; FILL mode writes the records at the scanned positions,
+// taking the same decisions.
+struct NearArgs {
+  int nboxes, ns, iperiod0;
+  double bs0, dmax;
+  const int *l1_ptr, *l1_src, *s_lo, *s_hi, *t_lo, *t_hi, *level;
+  const double *center, *soff;
+  const float* q;                 // FILL: charges of density 0
+  int* cnt;                       // COUNT: kept sources per list entry
+  unsigned long long* total;      // COUNT: sum of cnt
+  const int* pos;                 // FILL: first record of every list entry
+  float4* rec;                    // FILL: 4 float4 per kept source
+};
+
+template <int DIM, bool FILL>
+__global__ void k_near_lists(NearArgs n) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < n.nboxes; b += nw) {
+    const int e0 = n.l1_ptr[b], e1 = n.l1_ptr[b + 1];
+    const bool has_pts = (n.s_hi[b] > n.s_lo[b]) || (n.t_hi[b] > n.t_lo[b]);
+    double cT[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; k++) cT[k] = n.center[(size_t)b * DIM + k];
+    const double hT = 0.5 * n.bs0 * ldexp(1.0, -n.level[b]);
+    unsigned long long tot = 0;
+    for (int li = e0; li < e1; li++) {
+      int kept = 0;
+      const int sbx = n.l1_src[li];
+      double dc[DIM];
+#pragma unroll
+      for (int k = 0; k < DIM; k++) {
+        const double cs = n.center[(size_t)sbx * DIM + k];
+        double sh = 0;
+        if (n.iperiod0 == 1) {  // pfgt_find_local_shift, src/pfgt/pfgt_direct.f:620-651
+          double dx = cT[k] - cs, dxp1 = dx - n.bs0, dxm1 = dx + n.bs0;
+          if (fabs(dx) > fabs(dxp1)) { dx = dxp1; sh = n.bs0; }
+          if (fabs(dx) > fabs(dxm1)) sh = -n.bs0;
+        }
+        dc[k] = (cs + sh) - cT[k];
+      }
+      if (has_pts &&
+          !box_beyond_cutoff<DIM>(dc, hT + 0.5 * n.bs0 * ldexp(1.0, -n.level[sbx]), n.dmax)) {
+        const int s0 = n.s_lo[sbx], s1 = n.s_hi[sbx];
+        const int out = FILL ? n.pos[li] : 0;
+        for (int base = s0; base < s1; base += 32) {
+          const int j = base + lane;
+          double v[DIM];
+          bool keep = false;
+          if (j < s1) {
+#pragma unroll
+            for (int k = 0; k < DIM; k++) v[k] = n.soff[(size_t)k * n.ns + j] + dc[k];
+            keep = !box_beyond_cutoff<DIM>(v, hT, n.dmax);
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, keep);
+          if (FILL && keep) {
+            float h[3] = {0.f, 0.f, 0.f}, l[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int k = 0; k < DIM; k++) {
+              h[k] = (float)v[k];
+              l[k] = (float)(v[k] - (double)h[k]);
+            }
+            const float qv = n.q[j];
+            float4* r = n.rec + 4 * (size_t)(out + kept + __popc(m & ((1u << lane) - 1u)));
+            r[0] = make_float4(-h[0], -h[0], -h[1], -h[1]);
+            r[1] = make_float4(-h[2], -h[2], qv, qv);
+            r[2] = make_float4(-l[0], -l[0], -l[1], -l[1]);
+            r[3] = make_float4(-l[2], -l[2], 0.f, 0.f);
+          }
+          kept += __popc(m);
+        }
+      }
+      if (!FILL && lane == 0) n.cnt[li] = kept;
+      tot += kept;
+    }
+    if (!FILL && lane == 0 && tot) atomicAdd(n.total, tot);
+  }
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// k_direct32x2 on packed list-1 sources: a warp item is 64 points of one
+// target box; the box's records are streamed in batches of 32 sources
+// through a double-buffered shared-memory stage filled by asynchronous
+// 16-byte copies (the next batch lands while the current one is summed).
+// Items are taken from a device counter, the next index fetched while the
+// current item runs.  Pair arithmetic as k_direct32x2.
+template <int DIM, int PGH>
+__global__ void __launch_bounds__(DW * 32) k_direct32x2p(DArgs<float> a, const int* __restrict__ pos,
+                                                         const float4* __restrict__ rec,
+                                                         int* __restrict__ next) {
+  constexpr int NC = 1 + (PGH >= 2 ? DIM : 0);
+  __shared__ __align__(16) float4 stage[DW][2][32 * 4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const float ce = a.dinv * 1.4426950408889634f;  // exp(-rr/delta) = 2^(-rr*ce)
+  const float2 nce = make_float2(-ce, -ce), nrf = make_float2(-a.rfac, -a.rfac);
+  const int n_items = *a.n_items_dev;
+  int it = 0;
+  if (lane == 0) it = atomicAdd(next, 1);
+  it = __shfl_sync(0xffffffffu, it, 0);
+  while (it < n_items) {
+    int nxt = 0;
+    if (lane == 0) nxt = atomicAdd(next, 1);
+    const int tb = a.item_box[it];
+    const int pA = a.item_lo[it] + lane, pB = pA + 32;
+    const int ehi = a.e_hi[tb];
+    const bool actA = pA < ehi, actB = pB < ehi;
+    const int c0 = pos[a.l1_ptr[tb]], c1 = pos[a.l1_ptr[tb + 1]];
+    // first batch in flight before the target set-up
+    if (c0 + lane < c1) {
+      const float4* g = rec + 4 * (size_t)(c0 + lane);
+#pragma unroll
+      for (int r = 0; r < 4; r++) cp_async16(&stage[warp][0][4 * lane + r], g + r);
+    }
+    cp_async_commit();
+    float2 tx[3], txl[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      tx[k] = make_float2(0.f, 0.f);
+      txl[k] = make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int k = 0; k < DIM; k++) {
+      const double vA = actA ? a.eoff[(size_t)k * a.ne + pA] : 0.0;
+      const double vB = actB ? a.eoff[(size_t)k * a.ne + pB] : 0.0;
+      const float hA = (float)vA, hB = (float)vB;
+      tx[k] = make_float2(hA, hB);
+      txl[k] = make_float2((float)(vA - (double)hA), (float)(vB - (double)hB));
+    }
+    float2 acc[NC];
+    double accA[NC], accB[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      acc[c] = make_float2(0.f, 0.f);
+      accA[c] = 0.0;
+      accB[c] = 0.0;
+    }
+    int buf = 0;
+    for (int base = c0; base < c1; base += 32, buf ^= 1) {
+      // issue the next batch into the other buffer, then wait for this one
+      const int nb = base + 32;
+      if (nb + lane < c1) {
+        const float4* g = rec + 4 * (size_t)(nb + lane);
+#pragma unroll
+        for (int r = 0; r < 4; r++) cp_async16(&stage[warp][buf ^ 1][4 * lane + r], g + r);
+      }
+      cp_async_commit();
+      cp_async_wait1();
+      __syncwarp();
+      const float4* S = stage[warp][buf];
+      const int cnt = min(32, c1 - base);
+#pragma unroll 4
+      for (int jj = 0; jj < cnt; jj++) {
+        const float4 A = S[4 * jj], Bq = S[4 * jj + 1], Cl = S[4 * jj + 2], Dl = S[4 * jj + 3];
+        const float2 nh[3] = {make_float2(A.x, A.y), make_float2(A.z, A.w), make_float2(Bq.x, Bq.y)};
+        const float2 nl[3] = {make_float2(Cl.x, Cl.y), make_float2(Cl.z, Cl.w), make_float2(Dl.x, Dl.y)};
+        float2 dr[DIM], rr = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < DIM; k++) {
+          dr[k] = __fadd2_rn(__fadd2_rn(tx[k], nh[k]), __fadd2_rn(txl[k], nl[k]));
+          rr = __ffma2_rn(dr[k], dr[k], rr);
+        }
+        const float2 arg = __fmul2_rn(rr, nce);
+        const float eA = rr.x < a.dmax ? fgt_ex2(arg.x) : 0.f;
+        const float eB = rr.y < a.dmax ? fgt_ex2(arg.y) : 0.f;
+        const float2 r = __fmul2_rn(make_float2(eA, eB), make_float2(Bq.z, Bq.w));
+        acc[0] = __fadd2_rn(acc[0], r);
+        if (PGH >= 2) {
+          // gnd_directcg, src/pfgt/pfgt_direct.f:98-140: grad += -2/delta (t - s) r
+          const float2 rg = __fmul2_rn(r, nrf);
+#pragma unroll
+          for (int k = 0; k < DIM; k++) acc[1 + k] = __ffma2_rn(dr[k], rg, acc[1 + k]);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        accA[c] += (double)acc[c].x;
+        accB[c] += (double)acc[c].y;
+        acc[c] = make_float2(0.f, 0.f);
+      }
+      __syncwarp();  // this buffer is refilled two batches on
+    }
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      double* o = a.out + ((size_t)c * a.nd + a.d0) * a.ne;
+      if (actA) o[pA] += accA[c];
+      if (actB) o[pB] += accB[c];
+    }
+    it = __shfl_sync(0xffffffffu, nxt, 0);
+  }
+}
+
 __global__ void k_items_count(int nboxes, const int* __restrict__ l1_ptr, const int* __restrict__ lo,
                               const int* __restrict__ hi, const int* __restrict__ s_lo,
                               const int* __restrict__ s_hi, const int* __restrict__ l1_src,
@@ -593,9 +800,98 @@ void dispatch_dim(const DArgs<T>& a, int dim, int pgh, bool chg, bool dip, cudaS
 
 }  // namespace
 
+namespace {
+NearArgs near_args(const DirectGeom& g, const Lists& L, const int* s_lo, const int* s_hi,
+                   const int* t_lo, const int* t_hi, const double* soff, int ns) {
+  NearArgs n{};
+  n.nboxes = g.nboxes;
+  n.ns = ns;
+  n.iperiod0 = g.iperiod0;
+  n.bs0 = g.bs0;
+  n.dmax = g.dmax;
+  n.l1_ptr = L.l1_ptr;
+  n.l1_src = L.l1_src;
+  n.s_lo = s_lo;
+  n.s_hi = s_hi;
+  n.t_lo = t_lo;
+  n.t_hi = t_hi;
+  n.level = g.level;
+  n.center = g.center;
+  n.soff = soff;
+  return n;
+}
+template <bool FILL>
+void launch_near_lists(int dim, const NearArgs& n, cudaStream_t s) {
+  const int grid = grid_for((long long)n.nboxes * 32, 256);
+  if (dim == 1) k_near_lists<1, FILL><<<grid, 256, 0, s>>>(n);
+  else if (dim == 2) k_near_lists<2, FILL><<<grid, 256, 0, s>>>(n);
+  else k_near_lists<3, FILL><<<grid, 256, 0, s>>>(n);
+  FGT_LAUNCH_CHECK();
+}
+}  // namespace
+
+long long near_lists_count(const DirectGeom& g, const Lists& L, const int* s_lo, const int* s_hi,
+                           const int* t_lo, const int* t_hi, const double* soff, int ns,
+                           long long max_records, DBuf<int>& pos, cudaStream_t s) {
+  if (L.n_l1 <= 0) return -1;
+  NearArgs n = near_args(g, L, s_lo, s_hi, t_lo, t_hi, soff, ns);
+  DBuf<int> cnt(L.n_l1, s);
+  DBuf<unsigned long long> tot(1, s);
+  tot.zero();
+  n.cnt = cnt;
+  n.total = tot;
+  launch_near_lists<false>(g.dim, n, s);
+  unsigned long long h = 0;
+  FGT_CUDA(cudaMemcpyAsync(&h, tot.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+  FGT_CUDA(cudaStreamSynchronize(s));
+  if ((long long)h > max_records) return -1;
+  pos.alloc((size_t)L.n_l1 + 1, s);
+  exclusive_scan_i32(cnt, pos, L.n_l1, pos.get() + L.n_l1, s);
+  return (long long)h;
+}
+
+void near_lists_fill(const DirectGeom& g, const Lists& L, const SourceSet<float>& src,
+                     const int* t_lo, const int* t_hi, const int* pos, float4* rec,
+                     cudaStream_t s) {
+  NearArgs n = near_args(g, L, src.lo, src.hi, t_lo, t_hi, src.off, src.n);
+  n.q = src.q;
+  n.pos = pos;
+  n.rec = rec;
+  launch_near_lists<true>(g.dim, n, s);
+}
+
+namespace {
+// Blocks of k_direct32x2p resident on the device at once (the grid of the
+// dynamically scheduled launch).
+template <int DIM, int PGH>
+int resident_blocks_p() {
+  static int nb = 0;
+  if (nb == 0) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_direct32x2p<DIM, PGH>, DW * 32, 0) !=
+            cudaSuccess ||
+        per_sm <= 0) {
+      (void)cudaGetLastError();
+      per_sm = 4;
+    }
+    int dev = 0, sms = kSMs;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+      (void)cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    nb = per_sm * sms;
+  }
+  return nb;
+}
+template <int DIM, int PGH>
+void launch_packed(const DArgs<float>& a, const NearPacked& p, int* next, cudaStream_t s) {
+  const int grid = std::max(1, std::min(ceil_div(a.n_items, DW), resident_blocks_p<DIM, PGH>()));
+  k_direct32x2p<DIM, PGH><<<grid, DW * 32, 0, s>>>(a, p.pos, p.rec, next);
+  FGT_LAUNCH_CHECK();
+}
+}  // namespace
+
 template <typename T>
 int direct_near_field(const DirectGeom& g, const Lists& L, const SourceSet<T>& src,
-                      const EvalSet<T>& e, double* pairs, cudaStream_t s) {
+                      const EvalSet<T>& e, double* pairs, cudaStream_t s, const NearPacked* packed) {
   if (e.pgh <= 0 || e.n <= 0 || L.n_l1 <= 0) return 0;
   int nb = g.nboxes, launches = 0;
   bool chg = src.q != nullptr, dip = src.ds != nullptr;
@@ -651,6 +947,23 @@ int direct_near_field(const DirectGeom& g, const Lists& L, const SourceSet<T>& s
   a.dmax_d = g.dmax;
   a.out = e.out;
   if constexpr (sizeof(T) == 4) {
+    if (paired && packed && packed->rec) {
+      a.d0 = 0;
+      DBuf<int> next(1, s);
+      next.zero();
+      const DArgs<float>& af = a;
+      if (g.dim == 1) {
+        if (e.pgh == 1) launch_packed<1, 1>(af, *packed, next, s);
+        else launch_packed<1, 2>(af, *packed, next, s);
+      } else if (g.dim == 2) {
+        if (e.pgh == 1) launch_packed<2, 1>(af, *packed, next, s);
+        else launch_packed<2, 2>(af, *packed, next, s);
+      } else {
+        if (e.pgh == 1) launch_packed<3, 1>(af, *packed, next, s);
+        else launch_packed<3, 2>(af, *packed, next, s);
+      }
+      return launches + 1;
+    }
     if (paired) {
       a.d0 = 0;
       const int grid = std::max(1, std::min(ceil_div(n_items, DW), kSMs * 16));
@@ -679,9 +992,11 @@ int direct_near_field(const DirectGeom& g, const Lists& L, const SourceSet<T>& s
 }
 
 template int direct_near_field<float>(const DirectGeom&, const Lists&, const SourceSet<float>&,
-                                      const EvalSet<float>&, double*, cudaStream_t);
+                                      const EvalSet<float>&, double*, cudaStream_t,
+                                      const NearPacked*);
 template int direct_near_field<double>(const DirectGeom&, const Lists&, const SourceSet<double>&,
-                                       const EvalSet<double>&, double*, cudaStream_t);
+                                       const EvalSet<double>&, double*, cudaStream_t,
+                                       const NearPacked*);
 
 }  // namespace fgt
 
