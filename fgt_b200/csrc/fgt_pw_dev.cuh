@@ -410,20 +410,30 @@ __device__ __forceinline__ void spread_point(const PWArgs<T>& a, T* B, const dou
 // Kernel values and their derivatives with respect to the point's original
 // coordinate: d/dx phi((x_c - x)/halfw) = phi * beta * z / (sqrt(1-z^2) halfw),
 // times the coordinate scale (a.dscale = scale / halfw).  Zero at |z| = 1.
-template <typename T, int W>
-__device__ __forceinline__ int kernel_row_d(const PWArgs<T>& a, double x, T* phi, T* dphi) {
+template <typename T>
+__device__ __forceinline__ void kernel_val_d(const PWArgs<T>& a, T f0, int j, T& phi, T& dphi) {
+  const T z = (f0 + (T)j) * a.inv_hw;
+  const T q = T(1) - z * z;
+  const T rq = q > T(0) ? Real<T>::rsqrt_(q) : T(0);
+  const T e = Real<T>::expm(Real<T>::div12(a.beta * (z * z), T(1) + q * rq));
+  phi = e;
+  dphi = e * (a.beta * a.dscale) * z * rq;
+}
+// First stencil cell of a coordinate and the offset f0 = i0 - x/dx of the
+// kernel argument (cell j of the stencil is at f0 + j grid spacings).
+template <typename T>
+__device__ __forceinline__ int kernel_start(const PWArgs<T>& a, double x, T& f0) {
   const double u = x * a.inv_dx_d;
   const int i0 = (int)ceil(u - a.hwdx_d);
-  const T f0 = (T)((double)i0 - u);
+  f0 = (T)((double)i0 - u);
+  return i0;
+}
+template <typename T, int W>
+__device__ __forceinline__ int kernel_row_d(const PWArgs<T>& a, double x, T* phi, T* dphi) {
+  T f0;
+  const int i0 = kernel_start<T>(a, x, f0);
 #pragma unroll
-  for (int j = 0; j < W; j++) {
-    const T z = (f0 + (T)j) * a.inv_hw;
-    const T q = T(1) - z * z;
-    const T rq = q > T(0) ? Real<T>::rsqrt_(q) : T(0);
-    const T e = Real<T>::expm(Real<T>::div12(a.beta * (z * z), T(1) + q * rq));
-    phi[j] = e;
-    dphi[j] = e * (a.beta * a.dscale) * z * rq;
-  }
+  for (int j = 0; j < W; j++) kernel_val_d<T>(a, f0, j, phi[j], dphi[j]);
   return i0;
 }
 
@@ -556,6 +566,107 @@ __device__ __forceinline__ void interp_grad_cells(const GV& B, const IX& ix, con
     v[2] = gy;
     v[3] = gz;
   }
+}
+
+// ------------------------------------------- 3D FP32 stencil on a shared grid
+// Compile-time loop: f(std::integral_constant<int, i>) for i = B .. E-1.
+template <int B, int E, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (B < E) {
+    f(std::integral_constant<int, B>{});
+    static_for<B + 1, E>(f);
+  }
+}
+// Shared-space load at a 32-bit shared address plus a compile-time byte
+// offset: one address register per stencil line, the cell offsets in the
+// load's immediate.
+template <int OFF>
+__device__ __forceinline__ float lds_f32(uint32_t a) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1+%2];" : "=f"(v) : "r"(a), "n"(OFF));
+  return v;
+}
+__device__ __forceinline__ float lds_f32(uint32_t a) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+  return v;
+}
+
+// line_sums for a line of a grid in shared memory starting at byte address la.
+template <int W>
+__device__ __forceinline__ void line_sums_smem(uint32_t la, float bref, const float* ph,
+                                               const float* dph, float& s0, float& s1) {
+  const float2 nb = make_float2(-bref, -bref);
+  float2 a0, a1;
+  {
+    const float2 b = __fadd2_rn(make_float2(lds_f32<0>(la), lds_f32<4>(la)), nb);
+    a0 = __fmul2_rn(b, make_float2(ph[0], ph[1]));
+    a1 = __fmul2_rn(b, make_float2(dph[0], dph[1]));
+  }
+  static_for<1, W / 2>([&](auto P) {
+    constexpr int j = 2 * decltype(P)::value;
+    const float2 b = __fadd2_rn(make_float2(lds_f32<4 * j>(la), lds_f32<4 * j + 4>(la)), nb);
+    a0 = __ffma2_rn(b, make_float2(ph[j], ph[j + 1]), a0);
+    a1 = __ffma2_rn(b, make_float2(dph[j], dph[j + 1]), a1);
+  });
+  if constexpr (W % 2 == 1) {
+    const float b = lds_f32<4 * (W - 1)>(la) - bref;
+    a0.x = fmaf(b, ph[W - 1], a0.x);
+    a1.x = fmaf(b, dph[W - 1], a1.x);
+  }
+  s0 = a0.x + a0.y;
+  s1 = a1.x + a1.y;
+}
+
+// interp_grad_point for a 3D FP32 grid in shared memory without wrap-around
+// (grid at shared byte address gb): the same sums over B - Bref, with the
+// stencil addresses advanced by one add per line and the x weights computed
+// as the rolled x loop reaches them (no register rotation).
+template <int W>
+__device__ __forceinline__ void interp_grad_point_s3(const PWArgs<float>& a, uint32_t gb,
+                                                     const double* x, float* v) {
+  const Geo& g = a.g;
+  float ph[2][W], dph[2][W];  // y and z rows
+  float f0x;
+  int s[3];
+  s[0] = kernel_start<float>(a, x[0], f0x);
+  s[1] = kernel_row_d<float, W>(a, x[1], ph[0], dph[0]);
+  s[2] = kernel_row_d<float, W>(a, x[2], ph[1], dph[1]);
+  const LinIdx<3, W> ix(g, s);
+  const uint32_t str0 = 4u * (uint32_t)g.str[0], str1 = 4u * (uint32_t)g.str[1];
+  const uint32_t a0 = gb + 4u * (uint32_t)(ix.o[0] + ix.o[1] + ix.o[2]);
+  const float bref = lds_f32(a0 + (W / 2) * (str0 + str1) + 4u * (W / 2));
+  float ksy = 0.f, ksz = 0.f;
+#pragma unroll
+  for (int j = 0; j < W; j++) ksy += ph[0][j];
+#pragma unroll
+  for (int j = 0; j < W; j++) ksz += ph[1][j];
+  float pot = 0.f, gx = 0.f, gy = 0.f, gz = 0.f, ksx = 0.f;
+  uint32_t ax = a0;
+#pragma unroll 1
+  for (int jx = 0; jx < W; jx++, ax += str0) {
+    float px, dpx;
+    kernel_val_d<float>(a, f0x, jx, px, dpx);
+    ksx += px;
+    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+    uint32_t ay = ax;
+#pragma unroll
+    for (int jy = 0; jy < W; jy++, ay += str1) {
+      float s0, s1;
+      line_sums_smem<W>(ay, bref, ph[1], dph[1], s0, s1);
+      t0 += ph[0][jy] * s0;
+      t1 += dph[0][jy] * s0;
+      t2 += ph[0][jy] * s1;
+    }
+    pot += px * t0;
+    gx += dpx * t0;
+    gy += px * t1;
+    gz += px * t2;
+  }
+  v[0] = pot + bref * ((ksx * ksy) * ksz);
+  v[1] = gx;
+  v[2] = gy;
+  v[3] = gz;
 }
 
 template <typename T, int DIM, int W, class GV>

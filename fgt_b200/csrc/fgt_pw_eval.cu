@@ -117,8 +117,21 @@ __device__ __forceinline__ void build_eval_grid(const PWArgs<T>& a, const T* L, 
 // order.  DERIV: one potential grid, gradients through the kernel derivative
 // (no hessians); otherwise one grid per output component (pot, grad_k,
 // hess_kl).
+// Threads of a k_eval_comp CTA: more warps share the SM's one grid for the
+// 3D FP32 derivative kernel on a shared grid at widths <= 9 (its stencil
+// needs fewer registers), 512 otherwise.
+#ifndef FGT_EVAL3_THREADS
+#define FGT_EVAL3_THREADS 512
+#endif
 template <typename T, int DIM, int W, bool GB, bool DERIV>
-__global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<T> p) {
+constexpr int eval_threads() {
+  return (std::is_same<T, float>::value && DIM == 3 && W <= 9 && !GB && DERIV) ? FGT_EVAL3_THREADS
+                                                                               : PW_THREADS;
+}
+
+template <typename T, int DIM, int W, bool GB, bool DERIV>
+__global__ void __launch_bounds__(eval_threads<T, DIM, W, GB, DERIV>())
+    k_eval_comp(PWArgs<T> a, EvalPtrs<T> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geo& g = a.g;
   const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
@@ -140,6 +153,10 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<
   load_tw(tif, a.tif, 2 * NF * G);
   load_tw(tih, a.tih, 2 * NH * G);
   __syncthreads();
+  // shared-space byte address of the grid (shared-memory grid variants)
+  const uint32_t grid_saddr =
+      (uint32_t)__cvta_generic_to_shared(smem_raw) + (uint32_t)eval_offset<T>(G, K);
+  (void)grid_saddr;
   const int nbox = p.nbox_dev ? *p.nbox_dev : p.nbox;
   // boxes in decreasing point count, each CTA takes the next one
   __shared__ int s_next;
@@ -170,24 +187,46 @@ __global__ void __launch_bounds__(PW_THREADS) k_eval_comp(PWArgs<T> a, EvalPtrs<
               order_cells<T, DIM, W>(a, offs, ne, c0, n, p.cell_bins, perm, ordtmp, bins, bws);
             else
               order_chunk<T, DIM, W>(a, offs, ne, c0, n, perm, ordtmp, ordcnt);
+            // the next point's offsets are loaded while the current one is
+            // interpolated; outputs are added with fire-and-forget atomics
+            // (one contribution per point here, so the sum is the plain add)
+            int pt_n = 0;
+            double x_n[DIM];
+            if (threadIdx.x < n) {
+              pt_n = c0 + perm[threadIdx.x];
+#pragma unroll
+              for (int k = 0; k < DIM; k++) x_n[k] = offs[(size_t)k * ne + pt_n];
+            }
             for (int i = threadIdx.x; i < n; i += blockDim.x) {
-              const int pt = c0 + perm[i];
+              const int pt = pt_n;
               double x[DIM];
 #pragma unroll
-              for (int k = 0; k < DIM; k++) x[k] = offs[(size_t)k * ne + pt] * a.scale_d;
+              for (int k = 0; k < DIM; k++) x[k] = x_n[k] * a.scale_d;
+              if (i + (int)blockDim.x < n) {
+                pt_n = c0 + perm[i + blockDim.x];
+#pragma unroll
+                for (int k = 0; k < DIM; k++) x_n[k] = offs[(size_t)k * ne + pt_n];
+              }
               if constexpr (DERIV) {
                 T v[1 + DIM];
-                interp_grad_point<T, DIM, W>(a, BV, x, v);
+                if constexpr (!GB && DIM == 3 && std::is_same<T, float>::value) {
+                  if (!g.wrap)
+                    interp_grad_point_s3<W>(a, grid_saddr, x, v);
+                  else
+                    interp_grad_point<T, DIM, W>(a, BV, x, v);
+                } else {
+                  interp_grad_point<T, DIM, W>(a, BV, x, v);
+                }
                 const int nc = set ? p.ncomp[1] : p.ncomp[0];
-                outs[(size_t)id * ne + pt] += (double)v[0];
+                atomicAdd(&outs[(size_t)id * ne + pt], (double)v[0]);
                 if (nc > 1) {
 #pragma unroll
                   for (int d = 0; d < DIM; d++)
-                    outs[((size_t)(1 + d) * p.nd + id) * ne + pt] += (double)v[1 + d];
+                    atomicAdd(&outs[((size_t)(1 + d) * p.nd + id) * ne + pt], (double)v[1 + d]);
                 }
               } else {
                 const T v = interp_point<T, DIM, W>(a, BV, x);
-                outs[((size_t)c * p.nd + id) * ne + pt] += (double)v;
+                atomicAdd(&outs[((size_t)c * p.nd + id) * ne + pt], (double)v);
               }
             }
             __syncthreads();
@@ -345,6 +384,168 @@ __global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal(PWArgs<T> a, EvalP
   }
 }
 
+// FP32 modal evaluation (potential, or potential + gradient) of the boxes
+// with few points: the sums of k_eval_modal, with the box's expansion
+// streamed through shared memory in chunks of whole rows (register
+// prefetch of the next chunk while the current one is summed), stored as
+// (w lr, w lr, -w li, w li) so that one 128-bit broadcast load and two packed
+// FP32x2 FMAs against the point's (er, ei, ei, er) give the complex product
+// of a mode.  Rows, lanes and the FP64 reduction as in k_eval_modal.
+constexpr int MODAL_CHUNK = 1024;  // modes per staged chunk (whole rows)
+template <int DIM>
+__host__ __device__ constexpr int modal32_ncg() { return 1 + DIM; }
+template <int DIM>
+size_t modal32_smem(int K, int pmax) {
+  const int NF = 2 * K + 1, NH = K + 1;
+  return sizeof(double) * (MODAL_THREADS / 32) * 32 * modal32_ncg<DIM>() +
+         sizeof(float4) * ((size_t)NH * pmax + 2 * MODAL_CHUNK) +
+         sizeof(float2) * ((size_t)(DIM - 1) * NF * pmax + NH);
+}
+
+template <int DIM, bool GRAD>
+__global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal32(PWArgs<float> a, EvalPtrs<float> p,
+                                                                int pmax) {
+  constexpr int NCG = modal32_ncg<DIM>();
+  constexpr int NW = MODAL_THREADS / 32;
+  const Geo& g = a.g;
+  const int K = g.K, NF = 2 * K + 1, NH = K + 1;
+  const int nrows = g.nexp / NH;
+  const int rpc = max(1, MODAL_CHUNK / NH);  // rows per chunk
+  const int nch = (nrows + rpc - 1) / rpc;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* red = reinterpret_cast<double*>(smem_raw);                 // [NW][32][NCG]
+  float4* Ez = reinterpret_cast<float4*>(red + (size_t)NW * 32 * NCG);  // [NH][pmax]
+  float4* Lb = Ez + (size_t)NH * pmax;                                // [2][MODAL_CHUNK]
+  float2* Exy = reinterpret_cast<float2*>(Lb + 2 * MODAL_CHUNK);      // [(DIM-1) NF][pmax]
+  float2* T2 = Exy + (size_t)(DIM - 1) * NF * pmax;                   // [NH] (t, t)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int kz = threadIdx.x; kz < NH; kz += blockDim.x) T2[kz] = make_float2(a.ts[K + kz], a.ts[K + kz]);
+  const int nbox = p.nbox_dev ? *p.nbox_dev : p.nbox;
+  for (int bi = blockIdx.x; bi < nbox; bi += gridDim.x) {
+    const int e = p.boxes[bi];
+    const int box = p.eval_box[e];
+    const int n0 = p.n[0] > 0 && p.ncomp[0] > 0 ? p.hi[0][box] - p.lo[0][box] : 0;
+    const int n1 = p.n[1] > 0 && p.ncomp[1] > 0 ? p.hi[1][box] - p.lo[1][box] : 0;
+    const int np = n0 + n1;  // <= pmax by the box split
+    __syncthreads();
+    // phase factors e^{i k x_d}: FP64 sincos, stored as FP32
+    for (int i = threadIdx.x; i < np * DIM * NF; i += blockDim.x) {
+      const int r = i / np, pi = i - r * np, d = r / NF, k = r - d * NF - K;
+      if (d == DIM - 1 && k < 0) continue;
+      const int set = pi < n0 ? 0 : 1;
+      const int pt = set ? p.lo[1][box] + pi - n0 : p.lo[0][box] + pi;
+      const double* offs = set ? p.off[1] : p.off[0];
+      const int ne = set ? p.n[1] : p.n[0];
+      const double x = offs[(size_t)d * ne + pt] * a.scale_d;
+      double sn, cs;
+      sincos(x * (double)k, &sn, &cs);
+      const float c = (float)cs, sv = (float)sn;
+      if (d == DIM - 1) Ez[(size_t)k * pmax + pi] = make_float4(c, sv, sv, c);
+      else Exy[(size_t)r * pmax + pi] = make_float2(c, sv);
+    }
+    for (int id = 0; id < p.nd; id++) {
+      const float2* L = reinterpret_cast<const float2*>(p.loc + ((size_t)e * p.nd + id) * 2 * g.nexp);
+      const int nsub = 32 / max(1, min(32, np));
+      const int S = NW * nsub;  // row streams
+      for (int p0 = 0; p0 < np; p0 += 32) {
+        const int npg = min(32, np - p0);
+        const int pi = p0 + lane % npg, sub = lane / npg;
+        const bool act = sub < nsub;
+        const int rs = warp * nsub + sub;
+        float v[NCG];
+#pragma unroll
+        for (int c = 0; c < NCG; c++) v[c] = 0.f;
+        // chunk 0 to shared memory; later chunks prefetched into registers
+        float2 pf[MODAL_CHUNK / MODAL_THREADS];
+        auto fetch = [&](int c) {
+          const int m0 = c * rpc * NH, m1 = min(g.nexp, m0 + rpc * NH);
+#pragma unroll
+          for (int j = 0; j < MODAL_CHUNK / MODAL_THREADS; j++) {
+            const int m = m0 + threadIdx.x + j * MODAL_THREADS;
+            pf[j] = m < m1 ? __ldg(L + m) : make_float2(0.f, 0.f);
+          }
+        };
+        auto stage = [&](int c, float4* buf) {
+          const int m0 = c * rpc * NH;
+#pragma unroll
+          for (int j = 0; j < MODAL_CHUNK / MODAL_THREADS; j++) {
+            const int mm = threadIdx.x + j * MODAL_THREADS;
+            const float w = ((m0 + mm) % NH) == 0 ? 1.f : 2.f;
+            buf[mm] = make_float4(w * pf[j].x, w * pf[j].x, -w * pf[j].y, w * pf[j].y);
+          }
+        };
+        __syncthreads();
+        fetch(0);
+        stage(0, Lb);
+        __syncthreads();
+        for (int c = 0; c < nch; c++) {
+          if (c + 1 < nch) fetch(c + 1);
+          const float4* Lc = Lb + (c & 1) * MODAL_CHUNK;
+          const int r0 = c * rpc, r1 = min(nrows, r0 + rpc);
+          if (act) {
+            for (int r = r0 + ((rs - r0) % S + S) % S; r < r1; r += S) {
+              const float4* Lr = Lc + (size_t)(r - r0) * NH;
+              const float4* Ep = Ez + pi;
+              float2 s0 = make_float2(0.f, 0.f), s1 = make_float2(0.f, 0.f);
+#pragma unroll 4
+              for (int kz = 0; kz < NH; kz++) {
+                const float4 L4 = Lr[kz];
+                const float4 e4 = Ep[(size_t)kz * pmax];
+                float2 pr = __fmul2_rn(make_float2(L4.x, L4.y), make_float2(e4.x, e4.y));
+                pr = __ffma2_rn(make_float2(L4.z, L4.w), make_float2(e4.z, e4.w), pr);
+                s0 = __fadd2_rn(s0, pr);
+                if (GRAD) s1 = __ffma2_rn(T2[kz], pr, s1);
+              }
+              int ki[2] = {0, 0};
+              if (DIM == 3) {
+                ki[0] = r / NF;
+                ki[1] = r - ki[0] * NF;
+              } else if (DIM == 2) {
+                ki[0] = r;
+              }
+              float pr = 1.f, pim = 0.f;  // phase of the row in the other dimensions
+#pragma unroll
+              for (int d = 0; d < DIM - 1; d++) {
+                const float2 cc = Exy[(size_t)(d * NF + ki[d]) * pmax + pi];
+                const float nr = pr * cc.x - pim * cc.y;
+                pim = pr * cc.y + pim * cc.x;
+                pr = nr;
+              }
+              const float t0r = pr * s0.x - pim * s0.y, t0i = pr * s0.y + pim * s0.x;
+              v[0] += t0r;
+              if (GRAD) {
+                const float t1i = pr * s1.y + pim * s1.x;
+#pragma unroll
+                for (int d = 0; d < DIM - 1; d++) v[1 + d] -= t0i * a.ts[ki[d]];
+                v[DIM] -= t1i;
+              }
+            }
+          }
+          if (c + 1 < nch) stage(c + 1, Lb + ((c + 1) & 1) * MODAL_CHUNK);
+          __syncthreads();
+        }
+#pragma unroll
+        for (int c = 0; c < NCG; c++) red[((size_t)warp * 32 + lane) * NCG + c] = (double)v[c];
+        __syncthreads();
+        const double s1 = (double)a.inv_sqd0;
+        for (int i = threadIdx.x; i < npg * NCG; i += blockDim.x) {
+          const int q = i / NCG, c = i - q * NCG, pj = p0 + q;
+          const int set = pj < n0 ? 0 : 1;
+          if (c >= (set ? p.ncomp[1] : p.ncomp[0])) continue;
+          double v2 = 0;
+          for (int w = 0; w < NW; w++)
+            for (int sb = 0; sb < nsub; sb++) v2 += red[((size_t)w * 32 + sb * npg + q) * NCG + c];
+          v2 *= c == 0 ? 1.0 : s1;
+          const int ne = set ? p.n[1] : p.n[0];
+          const int pt = set ? p.lo[1][box] + pj - n0 : p.lo[0][box] + pj;
+          double* outs = set ? p.out[1] : p.out[0];
+          outs[((size_t)c * p.nd + id) * ne + pt] += v2;
+        }
+      }
+    }
+  }
+}
+
 // box partition by evaluation-point count
 __global__ void k_eval_split(int n_eval, const int* __restrict__ eval_box, const int* __restrict__ lo0,
                              const int* __restrict__ hi0, const int* __restrict__ lo1,
@@ -381,7 +582,10 @@ int launch_eval_k(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t
     const long nb = a.g.G - W + 1;
     long nbins = 1;
     for (int d = 0; d < DIM; d++) nbins *= nb;
-    epk.cell_bins = (!a.g.wrap && nb > 0 && nbins <= NBINS_MAX) ? (int)nbins : 0;
+    // order_cells spreads the bins over whole rounds of the CTA's threads
+    const long nthr = eval_threads<T, DIM, W, false, DERIV>();
+    const long padded = (nbins + nthr - 1) / nthr * nthr;
+    epk.cell_bins = (!a.g.wrap && nb > 0 && padded <= NBINS_MAX) ? (int)nbins : 0;
   }
   if (gb) {
     gs.alloc((size_t)grid * a.g.bufsz, s);
@@ -391,11 +595,11 @@ int launch_eval_k(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t
   if (gb) {
     auto k = k_eval_comp<T, DIM, W, true, DERIV>;
     set_smem(k, sm);
-    k<<<grid, PW_THREADS, sm, s>>>(a, epk);
+    k<<<grid, eval_threads<T, DIM, W, true, DERIV>(), sm, s>>>(a, epk);
   } else {
     auto k = k_eval_comp<T, DIM, W, false, DERIV>;
     set_smem(k, sm);
-    k<<<grid, PW_THREADS, sm, s>>>(a, epk);
+    k<<<grid, eval_threads<T, DIM, W, false, DERIV>(), sm, s>>>(a, epk);
   }
   FGT_LAUNCH_CHECK();
   return 1;
@@ -530,7 +734,31 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
     ep.nbox_dev = counts.get() + 1;
     int grid = std::max(1, std::min(L.n_eval, kSMs * 8));
     size_t sm = modal_fix + modal_pt * (size_t)std::max(thr, 1);
-    if (P.dim == 1) {
+    bool done = false;
+    if constexpr (sizeof(T) == 4) {
+      // FP32 without hessians: the staged-expansion kernel
+      if (ep.ncomp_max <= 1 + P.dim && P.K + 1 <= MODAL_CHUNK) {
+        const bool grad = ep.ncomp_max > 1;
+        const int pm = std::max(thr, 1);
+        auto go = [&](auto kern, size_t smb) {
+          set_smem(kern, smb);
+          kern<<<grid, MODAL_THREADS, smb, s>>>(a, ep, pm);
+        };
+        if (P.dim == 1) {
+          const size_t smb = modal32_smem<1>(P.K, pm);
+          if (grad) go(k_eval_modal32<1, true>, smb); else go(k_eval_modal32<1, false>, smb);
+        } else if (P.dim == 2) {
+          const size_t smb = modal32_smem<2>(P.K, pm);
+          if (grad) go(k_eval_modal32<2, true>, smb); else go(k_eval_modal32<2, false>, smb);
+        } else {
+          const size_t smb = modal32_smem<3>(P.K, pm);
+          if (grad) go(k_eval_modal32<3, true>, smb); else go(k_eval_modal32<3, false>, smb);
+        }
+        done = true;
+      }
+    }
+    if (done) {
+    } else if (P.dim == 1) {
       set_smem(k_eval_modal<T, 1>, sm);
       k_eval_modal<T, 1><<<grid, MODAL_THREADS, sm, s>>>(a, ep, thr);
     } else if (P.dim == 2) {
