@@ -70,81 +70,176 @@ __device__ __forceinline__ void for_colleagues(const TV& tv, int b, int periodic
   }
 }
 
-// Closures of a level-(lc+1) box (coords cf) and a level-lc box (coords cc)
+// ---- modified list 1 of every target box (pfgt_compute_modified_list1,
+// src/common/tree_routs_nd.f:1063-1257, restated from the target side):
+//   * same level: leaf colleagues (self included);
+//   * coarser: leaf colleagues of the parent (levels 1 .. npwlevel-1) whose
+//     closure touches the box;
+//   * finer: leaf children of non-leaf colleagues touching the box.
+// One warp per target box: the candidates of each stage are resolved by the
+// lanes at once (one key search per lane), and the kept boxes are emitted in
+// candidate order by ballot and prefix count, so count and fill agree.
+template <int DIM>
+__device__ __forceinline__ void coords_of_d(const TV& tv, int b, uint32_t* c) {
+  const int l = tv.level[b];
+  const uint64_t key = tv.key[b];
+#pragma unroll
+  for (int k = 0; k < DIM; k++) c[k] = 0;
+  for (int j = 0; j < l; j++) {
+    const int dig = (int)((key >> (DIM * (l - 1 - j))) & ((1u << DIM) - 1));
+#pragma unroll
+    for (int k = 0; k < DIM; k++) c[k] = (c[k] << 1) | ((dig >> k) & 1);
+  }
+}
+template <int DIM>
+__device__ __forceinline__ int find_box_d(const TV& tv, int l, const uint32_t* c) {
+  uint64_t key = 0;
+  for (int j = 0; j < l; j++) {
+    int dig = 0;
+#pragma unroll
+    for (int k = 0; k < DIM; k++) dig |= ((c[k] >> (l - 1 - j)) & 1) << k;
+    key = (key << DIM) | (uint64_t)dig;
+  }
+  const int lo = tv.lev_start[l], n = tv.lev_start[l + 1] - lo;
+  const int i = dev_find(tv.key + lo, n, key);
+  return i < 0 ? -1 : lo + i;
+}
+// Closures of a level-(lf) box (coords cf) and a level-(lf-1) box (coords cc)
 // touch: the distance tests of src/common/tree_routs_nd.f:1181-1213,
 // 1226-1245 in units of half the finer box size (periodic minimum image
 // when `periodic`).
-__device__ __forceinline__ bool touch_levels(const TV& tv, const uint32_t* cf, int lf,
-                                             const uint32_t* cc, int periodic) {
-  long long P = 2ll << lf;
-  for (int k = 0; k < tv.dim; k++) {
+template <int DIM>
+__device__ __forceinline__ bool touch_levels_d(const uint32_t* cf, int lf, const uint32_t* cc,
+                                               int periodic) {
+  const long long P = 2ll << lf;
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < DIM; k++) {
     long long d = (long long)(2 * cf[k] + 1) - (long long)(4 * cc[k] + 2);
     if (d < 0) d = -d;
     if (periodic && P - d < d) d = P - d;
-    if (d > 3) return false;
+    ok = ok && d <= 3;
   }
-  return true;
+  return ok;
 }
-
-// Modified list 1 of target box T (pfgt_compute_modified_list1,
-// src/common/tree_routs_nd.f:1063-1257, restated from the target side).
-template <typename F>
-__device__ void for_list1(const TV& tv, int T, F add) {
-  int l = tv.level[T];
-  bool leafT = !tv.nonleaf[T];
-  if (l > tv.nlevend) return;
-  if (l == 0) {
-    if (leafT) add(T);
-    return;
-  }
-  if (!(leafT || l == tv.npwlevel)) return;
-  int per = tv.iperiod0;
-  // same level: leaf colleagues (self included)
-  for_colleagues(tv, T, per, [&](int S) {
-    if (!tv.nonleaf[S]) add(S);
-  });
-  if (!leafT) return;
-  uint32_t cT[FGT_MAXDIM];
-  coords_of(tv, T, cT);
-  // coarser leaf sources adjacent to T (sources at level l-1 >= 1, l-1 < npwlevel)
-  if (l - 1 >= 1 && l - 1 < tv.npwlevel) {
-    for_colleagues(tv, tv.parent[T], per, [&](int S) {
-      if (tv.nonleaf[S]) return;
-      uint32_t cS[FGT_MAXDIM];
-      coords_of(tv, S, cS);
-      if (touch_levels(tv, cT, l, cS, per)) add(S);
-    });
-  }
-  // finer leaf sources: leaf children of non-leaf colleagues touching T
-  if (l + 1 <= tv.nlevend) {
-    int mc = 1 << tv.dim;
-    for_colleagues(tv, T, per, [&](int J) {
-      if (!tv.nonleaf[J]) return;
-      int c0 = tv.child0[J];
-      if (c0 < 0) return;
-      for (int j = 0; j < mc; j++) {
-        int S = c0 + j;
-        if (tv.nonleaf[S]) continue;
-        uint32_t cS[FGT_MAXDIM];
-        coords_of(tv, S, cS);
-        if (touch_levels(tv, cS, l + 1, cT, per)) add(S);
+// Colleague `i` (in the candidate order of for_colleagues) of box b on this
+// lane: the box id, or -1 (no such box, or i >= *tot).
+template <int DIM>
+__device__ __forceinline__ int colleague_of(const TV& tv, int b, int periodic, int i, int* tot) {
+  const int l = tv.level[b];
+  uint32_t c[DIM];
+  coords_of_d<DIM>(tv, b, c);
+  const long long n = 1ll << l;
+  uint32_t vals[DIM][3];
+  int nv[DIM];
+#pragma unroll
+  for (int k = 0; k < DIM; k++) {
+    nv[k] = 0;
+#pragma unroll
+    for (int o = -1; o <= 1; o++) {
+      long long q = (long long)c[k] + o;
+      if (periodic) q = ((q % n) + n) % n;
+      else if (q < 0 || q >= n) continue;
+      bool dup = false;
+#pragma unroll
+      for (int j = 0; j < 3; j++) dup |= (j < nv[k] && vals[k][j] == (uint32_t)q);
+      if (!dup) {
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+          if (j == nv[k]) vals[k][j] = (uint32_t)q;
+        nv[k]++;
       }
-    });
+    }
+  }
+  int t = 1;
+#pragma unroll
+  for (int k = 0; k < DIM; k++) t *= nv[k];
+  *tot = t;
+  if (i >= t) return -1;
+  uint32_t q[DIM];
+  int r = i;
+#pragma unroll
+  for (int k = 0; k < DIM; k++) {
+    const int s = r % nv[k];
+    q[k] = s == 0 ? vals[k][0] : (s == 1 ? vals[k][1] : vals[k][2]);
+    r /= nv[k];
+  }
+  return find_box_d<DIM>(tv, l, q);
+}
+
+template <int DIM, bool FILL>
+__global__ void k_list1_warp(TV tv, int nboxes, int* __restrict__ cnt, const int* __restrict__ ptr,
+                             int* __restrict__ out) {
+  constexpr int MC = 1 << DIM;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int T = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; T < nboxes; T += nw) {
+    const int base = FILL ? ptr[T] : 0;
+    int n = 0;
+    auto emit = [&](bool keep, int S) {
+      const unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (FILL && keep) out[base + n + __popc(m & lt)] = S;
+      n += __popc(m);
+    };
+    const int l = tv.level[T];
+    const bool leafT = !tv.nonleaf[T];
+    if (l <= tv.nlevend) {
+      if (l == 0) {
+        emit(lane == 0 && leafT, T);
+      } else if (leafT || l == tv.npwlevel) {
+        const int per = tv.iperiod0;
+        // same level: leaf colleagues (self included)
+        int tot1;
+        const int J = colleague_of<DIM>(tv, T, per, lane, &tot1);
+        emit(J >= 0 && !tv.nonleaf[J], J);
+        if (leafT) {
+          uint32_t cT[DIM];
+          coords_of_d<DIM>(tv, T, cT);
+          // coarser leaf sources adjacent to T
+          if (l - 1 >= 1 && l - 1 < tv.npwlevel) {
+            int tot2;
+            const int S = colleague_of<DIM>(tv, tv.parent[T], per, lane, &tot2);
+            bool keep = false;
+            if (S >= 0 && !tv.nonleaf[S]) {
+              uint32_t cS[DIM];
+              coords_of_d<DIM>(tv, S, cS);
+              keep = touch_levels_d<DIM>(cT, l, cS, per);
+            }
+            emit(keep, S);
+          }
+          // finer leaf sources: leaf children of non-leaf colleagues touching T
+          if (l + 1 <= tv.nlevend) {
+            for (int c0 = 0; c0 < tot1 * MC; c0 += 32) {
+              const int c = c0 + lane, i = c / MC, j = c % MC;
+              const int Ji = __shfl_sync(0xffffffffu, J, i & 31);
+              bool keep = false;
+              int S = -1;
+              if (c < tot1 * MC && Ji >= 0 && tv.nonleaf[Ji] && tv.child0[Ji] >= 0) {
+                S = tv.child0[Ji] + j;
+                if (!tv.nonleaf[S]) {
+                  uint32_t cS[DIM];
+                  coords_of_d<DIM>(tv, S, cS);
+                  keep = touch_levels_d<DIM>(cS, l + 1, cT, per);
+                }
+              }
+              emit(keep, S);
+            }
+          }
+        }
+      }
+    }
+    if (!FILL && lane == 0) cnt[T] = n;
   }
 }
 
-__global__ void k_list1_count(TV tv, int nboxes, int* __restrict__ cnt) {
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nboxes; b += gridDim.x * blockDim.x) {
-    int c = 0;
-    for_list1(tv, b, [&](int) { c++; });
-    cnt[b] = c;
-  }
-}
-__global__ void k_list1_fill(TV tv, int nboxes, const int* __restrict__ ptr, int* __restrict__ out) {
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nboxes; b += gridDim.x * blockDim.x) {
-    int p = ptr[b];
-    for_list1(tv, b, [&](int S) { out[p++] = S; });
-  }
+template <bool FILL>
+void launch_list1(const TV& tv, int nb, int* cnt, const int* ptr, int* out, cudaStream_t s) {
+  const int grid = grid_for((long long)nb * 32, 256);
+  if (tv.dim == 1) k_list1_warp<1, FILL><<<grid, 256, 0, s>>>(tv, nb, cnt, ptr, out);
+  else if (tv.dim == 2) k_list1_warp<2, FILL><<<grid, 256, 0, s>>>(tv, nb, cnt, ptr, out);
+  else k_list1_warp<3, FILL><<<grid, 256, 0, s>>>(tv, nb, cnt, ptr, out);
+  FGT_LAUNCH_CHECK();
 }
 
 // Plane-wave flags at the cutoff level: form (npts > ndiv, pfgt.f:779) and
@@ -254,13 +349,11 @@ void build_lists(const Tree& t, int npwlevel, int iperiod0, int nlevend, bool do
   L.l1_ptr.alloc(nb + 1, s);
   {
     DBuf<int> cnt(nb, s), tot(1, s);
-    k_list1_count<<<grid_for(nb, 128), 128, 0, s>>>(tv, nb, cnt);
-    FGT_LAUNCH_CHECK();
+    launch_list1<false>(tv, nb, cnt, nullptr, nullptr, s);
     exclusive_scan_i32(cnt, L.l1_ptr, nb, L.l1_ptr.get() + nb, s);
     L.n_l1 = fetch_int(L.l1_ptr.get() + nb, s);
     L.l1_src.alloc(std::max(L.n_l1, 1), s);
-    k_list1_fill<<<grid_for(nb, 128), 128, 0, s>>>(tv, nb, L.l1_ptr, L.l1_src);
-    FGT_LAUNCH_CHECK();
+    launch_list1<true>(tv, nb, nullptr, L.l1_ptr, L.l1_src, s);
   }
   L.n_form = L.n_eval = L.n_trans = 0;
   if (!do_pw) return;

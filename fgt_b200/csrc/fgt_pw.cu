@@ -345,29 +345,36 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
 }
 
 // ---------------------------------------------------------------- translate
+// Local expansion of every eval box: its own form expansion plus the
+// diagonal translations W[w] * M[s] of its list (gnd_shiftpw,
+// src/pfgt/bfgt_pwrouts.f:1555-1636), one mode per thread, complex values
+// as 8- or 16-byte vectors.
 template <typename T>
-__global__ void k_translate(int n_eval, int nexp, int nd, const int* __restrict__ self,
+__global__ void k_translate(int n_eval, int nexp, int nd, int ge, const int* __restrict__ self,
                             const int* __restrict__ ptr, const int* __restrict__ src,
                             const int* __restrict__ widx, const T* __restrict__ mp,
                             const T* __restrict__ wtab, T* __restrict__ loc) {
-  const int e = blockIdx.y;
+  using V = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+  const V* mpv = reinterpret_cast<const V*>(mp);
+  const V* wv = reinterpret_cast<const V*>(wtab);
+  V* lv = reinterpret_cast<V*>(loc);
+  const int e0 = blockIdx.y * ge, e1 = min(n_eval, e0 + ge);
   for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < nexp; m += gridDim.x * blockDim.x) {
-    for (int id = 0; id < nd; id++) {
-      T re = T(0), im = T(0);
-      const int sf = self[e];
-      if (sf >= 0) {
-        re = mp[(((size_t)sf * nd + id) * nexp + m) * 2];
-        im = mp[(((size_t)sf * nd + id) * nexp + m) * 2 + 1];
+    for (int e = e0; e < e1; e++) {
+      const int sf = self[e], j0 = ptr[e], j1 = ptr[e + 1];
+      for (int id = 0; id < nd; id++) {
+        V acc;
+        acc.x = T(0);
+        acc.y = T(0);
+        if (sf >= 0) acc = __ldg(mpv + ((size_t)sf * nd + id) * nexp + m);
+        for (int j = j0; j < j1; j++) {
+          const V av = __ldg(mpv + ((size_t)src[j] * nd + id) * nexp + m);
+          const V w = __ldg(wv + (size_t)widx[j] * nexp + m);
+          acc.x += av.x * w.x - av.y * w.y;
+          acc.y += av.x * w.y + av.y * w.x;
+        }
+        lv[((size_t)e * nd + id) * nexp + m] = acc;
       }
-      for (int j = ptr[e]; j < ptr[e + 1]; j++) {
-        const size_t mi = (((size_t)src[j] * nd + id) * nexp + m) * 2;
-        const size_t wi = ((size_t)widx[j] * nexp + m) * 2;
-        const T ar = mp[mi], ai = mp[mi + 1], wr = wtab[wi], wi_ = wtab[wi + 1];
-        re += ar * wr - ai * wi_;
-        im += ar * wi_ + ai * wr;
-      }
-      loc[(((size_t)e * nd + id) * nexp + m) * 2] = re;
-      loc[(((size_t)e * nd + id) * nexp + m) * 2 + 1] = im;
     }
   }
 }
@@ -655,11 +662,14 @@ int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, PWWork* work, 
     work->bytes_translate = (double)sizeof(T) * 2 * P.nexp * P.nd *
                             ((double)L.n_trans + 2.0 * L.n_eval);
   if (L.n_eval == 0) return 1;
+  // a thread runs one mode of TGE consecutive eval boxes, which share most
+  // of their source expansions: the repeated reads hit L1
+  constexpr int TGE = 4;
   int gx = std::max(1, std::min(ceil_div(P.nexp, 256), 64));
-  for (int e0 = 0; e0 < L.n_eval; e0 += 65535) {
-    int ne = std::min(65535, L.n_eval - e0);
-    dim3 grid(gx, ne);
-    k_translate<T><<<grid, 256, 0, s>>>(ne, P.nexp, P.nd, L.eval_self.get() + e0,
+  for (int e0 = 0; e0 < L.n_eval; e0 += 65535 * TGE) {
+    int ne = std::min(65535 * TGE, L.n_eval - e0);
+    dim3 grid(gx, ceil_div(ne, TGE));
+    k_translate<T><<<grid, 256, 0, s>>>(ne, P.nexp, P.nd, TGE, L.eval_self.get() + e0,
                                         L.trans_ptr.get() + e0, L.trans_src, L.trans_w, D.mp,
                                         D.wtab, D.loc.get() + (size_t)e0 * P.nd * 2 * P.nexp);
     FGT_LAUNCH_CHECK();

@@ -16,18 +16,22 @@ struct KeyParams {
   double bsh[64];  // bsh[l] = boxsize(l+1)/2: child-centre offset below level l
 };
 
-__global__ void k_bbox(const double* __restrict__ x, int n, int dim, double* __restrict__ part) {
-  double lo[FGT_MAXDIM], hi[FGT_MAXDIM];
-  for (int k = 0; k < dim; k++) { lo[k] = INFINITY; hi[k] = -INFINITY; }
+template <int DIM>
+__global__ void k_bbox(const double* __restrict__ x, int n, double* __restrict__ part) {
+  double lo[DIM], hi[DIM];
+#pragma unroll
+  for (int k = 0; k < DIM; k++) { lo[k] = INFINITY; hi[k] = -INFINITY; }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    for (int k = 0; k < dim; k++) {
-      double v = x[(size_t)i * dim + k];
+#pragma unroll
+    for (int k = 0; k < DIM; k++) {
+      double v = x[(size_t)i * DIM + k];
       lo[k] = fmin(lo[k], v);
       hi[k] = fmax(hi[k], v);
     }
-  __shared__ double slo[FGT_MAXDIM][32], shi[FGT_MAXDIM][32];
+  __shared__ double slo[DIM][32], shi[DIM][32];
   int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int k = 0; k < dim; k++) {
+#pragma unroll
+  for (int k = 0; k < DIM; k++) {
     double a = lo[k], b = hi[k];
     for (int o = 16; o; o >>= 1) {
       a = fmin(a, __shfl_xor_sync(0xffffffffu, a, o));
@@ -37,11 +41,12 @@ __global__ void k_bbox(const double* __restrict__ x, int n, int dim, double* __r
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int k = 0; k < dim; k++) {
+#pragma unroll
+    for (int k = 0; k < DIM; k++) {
       double a = INFINITY, b = -INFINITY;
       for (int j = 0; j < (int)(blockDim.x >> 5); j++) { a = fmin(a, slo[k][j]); b = fmax(b, shi[k][j]); }
-      part[(size_t)blockIdx.x * 2 * dim + k] = a;
-      part[(size_t)blockIdx.x * 2 * dim + dim + k] = b;
+      part[(size_t)blockIdx.x * 2 * DIM + k] = a;
+      part[(size_t)blockIdx.x * 2 * DIM + DIM + k] = b;
     }
   }
 }
@@ -51,23 +56,40 @@ __global__ void k_bbox(const double* __restrict__ x, int n, int dim, double* __r
 // of tree_refine_boxes (src/common/tree_routs_nd.f:42-45) and
 // find_childbox_ind (src/common/pts_tree_nd.f:733-737), so box membership is
 // bit-identical to the reference.
+template <int DIM>
 __global__ void k_point_keys(const double* __restrict__ x, int n, KeyParams p,
                              uint64_t* __restrict__ keys) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double c[FGT_MAXDIM], xi[FGT_MAXDIM];
-    for (int k = 0; k < p.dim; k++) { c[k] = p.cen0[k]; xi[k] = x[(size_t)i * p.dim + k]; }
+    double c[DIM], xi[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; k++) { c[k] = p.cen0[k]; xi[k] = x[(size_t)i * DIM + k]; }
     uint64_t key = 0;
     for (int l = 0; l < p.D; l++) {
       int dig = 0;
-      for (int k = 0; k < p.dim; k++) {
+      const double h = p.bsh[l];
+#pragma unroll
+      for (int k = 0; k < DIM; k++) {
         bool up = (xi[k] - c[k] >= 0);
         dig |= (up ? 1 : 0) << k;
-        c[k] = c[k] + (up ? p.bsh[l] : -p.bsh[l]);
+        c[k] = c[k] + (up ? h : -h);
       }
-      key = (key << p.dim) | (uint64_t)dig;
+      key = (key << DIM) | (uint64_t)dig;
     }
     keys[i] = key;
   }
+}
+void launch_point_keys(int dim, const double* x, int n, const KeyParams& p, uint64_t* keys,
+                       cudaStream_t s) {
+  if (dim == 1) k_point_keys<1><<<grid_for(n, 256), 256, 0, s>>>(x, n, p, keys);
+  else if (dim == 2) k_point_keys<2><<<grid_for(n, 256), 256, 0, s>>>(x, n, p, keys);
+  else k_point_keys<3><<<grid_for(n, 256), 256, 0, s>>>(x, n, p, keys);
+  FGT_LAUNCH_CHECK();
+}
+void launch_bbox(int dim, const double* x, int n, int gb, double* part, cudaStream_t s) {
+  if (dim == 1) k_bbox<1><<<gb, 256, 0, s>>>(x, n, part);
+  else if (dim == 2) k_bbox<2><<<gb, 256, 0, s>>>(x, n, part);
+  else k_bbox<3><<<gb, 256, 0, s>>>(x, n, part);
+  FGT_LAUNCH_CHECK();
 }
 
 // Source count of each box of level l from the sorted full keys.
@@ -255,10 +277,8 @@ void tree_setup_scalars(int dim, double delta, double eps, int iperiod, const do
   if (iperiod != 1) {
     int gb = 4 * kSMs;
     DBuf<double> part((size_t)2 * gb * 2 * dim, s);
-    k_bbox<<<gb, 256, 0, s>>>(d_src, ns, dim, part.get());
-    FGT_LAUNCH_CHECK();
-    k_bbox<<<gb, 256, 0, s>>>(d_trg, nt, dim, part.get() + (size_t)gb * 2 * dim);
-    FGT_LAUNCH_CHECK();
+    launch_bbox(dim, d_src, ns, gb, part.get(), s);
+    launch_bbox(dim, d_trg, nt, gb, part.get() + (size_t)gb * 2 * dim, s);
     std::vector<double> h((size_t)2 * gb * 2 * dim);
     FGT_CUDA(cudaMemcpyAsync(h.data(), part.get(), sizeof(double) * h.size(),
                              cudaMemcpyDeviceToHost, s));
@@ -323,14 +343,8 @@ void tree_build(Tree& t, int dim, int iperiod, int npwlevel, int ndiv, double bs
   }
   // 1. full keys of sources and targets
   DBuf<uint64_t> skey(ns, s), tkey(nt, s), ksorted(ns, s), ktmp(std::max(ns, nt), s);
-  if (ns > 0) {
-    k_point_keys<<<grid_for(ns, 256), 256, 0, s>>>(d_src, ns, kp, skey);
-    FGT_LAUNCH_CHECK();
-  }
-  if (nt > 0) {
-    k_point_keys<<<grid_for(nt, 256), 256, 0, s>>>(d_trg, nt, kp, tkey);
-    FGT_LAUNCH_CHECK();
-  }
+  if (ns > 0) launch_point_keys(dim, d_src, ns, kp, skey, s);
+  if (nt > 0) launch_point_keys(dim, d_trg, nt, kp, tkey, s);
   if (ns > 0)
     FGT_CUDA(cudaMemcpyAsync(ksorted.get(), skey.get(), sizeof(uint64_t) * ns,
                              cudaMemcpyDeviceToDevice, s));
