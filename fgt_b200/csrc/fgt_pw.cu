@@ -45,7 +45,7 @@ constexpr int TP = 12;          // padded kernel row (TILE <= TP - 1)
 // twiddle tables, rounded up to 16 bytes (the tiled scratch follows)
 template <typename T>
 __host__ __device__ constexpr size_t tw_bytes16(int G, int K) {
-  return ((size_t)sizeof(T) * 2 * G * ((2 * K + 1) + (K + 1)) + 15) & ~(size_t)15;
+  return ((size_t)sizeof(T) * tw_elems(G, K) + 15) & ~(size_t)15;
 }
 // byte offset of the grid buffer in the tiled form kernel; every part is a
 // multiple of 16 bytes, so the kernel-row buffer is float4 aligned
@@ -216,10 +216,11 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
   const Geo& g = a.g;
   const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
   T* sm = reinterpret_cast<T*>(smem_raw);
-  T* twf = sm;                // G*NF complex
-  T* twh = twf + 2 * G * NF;  // G*NH complex
+  const int NFp = pad4(NF), NHp = pad4(NH);
+  T* twf = sm;                 // G*NF complex, planar rows of 2*NFp
+  T* twh = twf + 2 * G * NFp;  // G*NH complex, planar rows of 2*NHp
   // atomic-spreading scratch
-  int* ordtmp = reinterpret_cast<int*>(twh + 2 * G * NH);  // ORDER_CHUNK
+  int* ordtmp = reinterpret_cast<int*>(sm + tw_elems(G, K));  // ORDER_CHUNK
   int* ordcnt = ordtmp + ORDER_CHUNK;                        // 32
   unsigned short* perm = reinterpret_cast<unsigned short*>(ordcnt + 32);  // ORDER_CHUNK
   // tiled-spreading scratch
@@ -232,8 +233,8 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
   T* B = GB ? a.gscratch + (size_t)blockIdx.x * g.bufsz
             : reinterpret_cast<T*>(smem_raw + (TILED ? tiled_offset<T>(G, K)
                                                      : order_offset<T>(G, K)));
-  load_tw(twf, a.twf, 2 * G * NF);
-  load_tw(twh, a.twh, 2 * G * NH);
+  load_tw(twf, a.twf, 2 * G * NFp);
+  load_tw(twh, a.twh, 2 * G * NHp);
   __syncthreads();
   // boxes in decreasing source count, each CTA takes the next one
   __shared__ int s_next;
@@ -303,13 +304,13 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
           if (DIM == 1) {
             for (int l = 0; l < G; l++) {
               const T gv = B[l];
-              re += gv * twh[2 * (l * NH + kxi)];
-              im += gv * twh[2 * (l * NH + kxi) + 1];
+              re += gv * twh[l * 2 * NHp + kxi];
+              im += gv * twh[l * 2 * NHp + NHp + kxi];
             }
           } else {
             for (int l = 0; l < G; l++) {
               const T xr = B[l * g.str[0] + lb], xi = B[l * g.str[0] + lb + 1];
-              const T tr = twf[2 * (l * NF + kxi)], ti = twf[2 * (l * NF + kxi) + 1];
+              const T tr = twf[l * 2 * NFp + kxi], ti = twf[l * 2 * NFp + NFp + kxi];
               re += xr * tr - xi * ti;
               im += xr * ti + xi * tr;
             }

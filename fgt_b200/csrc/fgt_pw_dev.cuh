@@ -45,7 +45,7 @@ struct PWArgs {
   Geo g;
   T halfw_over_dx, inv_hw, beta, dscale;  // inv_hw = dx / halfw
   double scale_d, inv_dx_d, hwdx_d;  // FP64 positions (points are FP64 offsets)
-  const T* twf;   // [G][2K+1] fwd full
+  const T* twf;   // [G][2K+1] fwd full (planar rows, see pad4)
   const T* twh;   // [G][K+1]  fwd half
   const T* tif;   // [2K+1][G] inv full
   const T* tih;   // [K+1][G]  inv half (with 1/2/2/.. weights)
@@ -56,12 +56,24 @@ struct PWArgs {
   T* gscratch;  // global buffer slices when the grid does not fit in smem
 };
 
+// Twiddle tables are planar per input index l: row l holds the real parts
+// of the nout outputs, zero-padded to a multiple of 4, then the imaginary
+// parts (so a thread's 4 consecutive outputs are two 128-bit loads).
+__host__ __device__ constexpr int pad4(int n) { return (n + 3) & ~3; }
+// elements of the staged tables of either kernel: form G x (2K+1) and
+// G x (K+1), evaluation (2K+1) x G and (K+1) x G, complex, planar rows
+__host__ __device__ constexpr size_t tw_elems(int G, int K) {
+  return 2 * (size_t)((size_t)G * (pad4(2 * K + 1) + pad4(K + 1)) > (size_t)pad4(G) * (3 * K + 2)
+                          ? (size_t)G * (pad4(2 * K + 1) + pad4(K + 1))
+                          : (size_t)pad4(G) * (3 * K + 2));
+}
+
 // byte offset of the grid buffer in shared memory: twiddles, then the
 // ordering scratch (ORDER_CHUNK ints + 32 counters + ORDER_CHUNK u16)
 template <typename T>
 __host__ __device__ constexpr size_t order_offset(int G, int K) {
-  return (((size_t)sizeof(T) * 2 * G * ((2 * K + 1) + (K + 1)) +
-           sizeof(int) * (ORDER_CHUNK + 32) + sizeof(unsigned short) * ORDER_CHUNK) + 15) &
+  return (((size_t)sizeof(T) * tw_elems(G, K) + sizeof(int) * (ORDER_CHUNK + 32) +
+           sizeof(unsigned short) * ORDER_CHUNK) + 15) &
          ~(size_t)15;
 }
 
@@ -73,60 +85,69 @@ __host__ __device__ constexpr size_t order_offset(int G, int K) {
 template <typename T, int MODE>
 __device__ __forceinline__ void pass_inplace(T* B, int nl, int nb, int SA, int SB, int ein,
                                              int eout, int nin, int nout, const T* __restrict__ tw) {
-  // register tile: LG lines x KG outputs per thread; a round covers whole
-  // lines (all of a line's inputs are read before any output is written)
-  constexpr int LG = 2, KG = sizeof(T) == 4 ? 4 : 2;
-  const int nkg = (nout + KG - 1) / KG;
-  const int ngroups = blockDim.x / nkg;
-  const int t = threadIdx.x, lg = t / nkg, kg = t - lg * nkg;
-  const bool act_t = lg < ngroups;
-  const int lpr = ngroups * LG;
+  constexpr int LG = 2;
+  static_assert(LG == 2, "two line pointers below");
+  const int np = pad4(nout);  // twiddle row: np real parts, then np imaginary parts
   if constexpr (std::is_same<T, float>::value) {
-    // FP32: complex accumulators as FP32x2 pairs (re, im); a complex MAC is
-    // two packed FMAs, (re, im) += (xr, xr)(tr, ti) + (xi, xi)(-ti, tr); the
-    // real-output pass accumulates (xr tr, -xi ti) and adds the halves.
+    // FP32: a thread owns LG lines x 4 consecutive outputs; the twiddles of
+    // its outputs are two 128-bit loads per input (real parts, imaginary
+    // parts), and the accumulators are FP32x2 pairs of neighbouring outputs,
+    // (re_k, re_k+1) += (xr, xr)(tr_k, tr_k+1) - (xi, xi)(ti_k, ti_k+1),
+    // (im_k, im_k+1) += (xr, xr)(ti_k, ti_k+1) + (xi, xi)(tr_k, tr_k+1).
+    // Lines past nl and outputs past nout compute on clamped or zero-padded
+    // data and are not stored.
+    const int nkg = np / 4;
+    const int ngroups = blockDim.x / nkg;
+    const int t = threadIdx.x, lg = t / nkg, kg = t - lg * nkg;
+    const bool act_t = lg < ngroups;
+    const int lpr = ngroups * LG;
+    const float4* twr = reinterpret_cast<const float4*>(tw) + kg;  // + l * (np / 2) per row
+    const int rstep = np / 2;                                       // float4 per row
     for (int r0 = 0; r0 < nl; r0 += lpr) {
-      float2 acc[LG][KG];
+      float2 ar[LG][2], ai[LG][2];
       int base[LG];
       bool lact[LG];
 #pragma unroll
       for (int g = 0; g < LG; g++) {
         const int line = r0 + lg * LG + g;
         lact[g] = act_t && line < nl;
-        base[g] = lact[g] ? (line / nb) * SA + (line % nb) * SB : 0;
+        const int lc = lact[g] ? line : 0;
+        base[g] = (lc / nb) * SA + (lc % nb) * SB;
 #pragma unroll
-        for (int j = 0; j < KG; j++) acc[g][j] = make_float2(0.f, 0.f);
+        for (int j = 0; j < 2; j++) {
+          ar[g][j] = make_float2(0.f, 0.f);
+          ai[g][j] = make_float2(0.f, 0.f);
+        }
       }
       if (act_t) {
-        for (int l = 0; l < nin; l++) {
-          float2 t1[KG], t2[KG];
-#pragma unroll
-          for (int j = 0; j < KG; j++) {
-            const int k = kg + j * nkg;  // interleaved: neighbouring lanes, neighbouring modes
-            const bool ok = k < nout;
-            const float tr = ok ? tw[2 * (l * nout + k)] : 0.f;
-            const float ti = ok ? tw[2 * (l * nout + k) + 1] : 0.f;
-            t1[j] = MODE == 2 ? make_float2(tr, -ti) : make_float2(tr, ti);
-            t2[j] = make_float2(-ti, tr);
-          }
+        const float4* tp = twr;
+        const float* bp0 = B + base[0];
+        const float* bp1 = B + base[LG - 1];
+#pragma unroll 2
+        for (int l = 0; l < nin; l++, tp += rstep, bp0 += ein, bp1 += ein) {
+          const float4 TR = tp[0], TI = tp[np / 4];  // real row, imaginary row
+          const float2 tr01 = make_float2(TR.x, TR.y), tr23 = make_float2(TR.z, TR.w);
+          const float2 ti01 = make_float2(TI.x, TI.y), ti23 = make_float2(TI.z, TI.w);
 #pragma unroll
           for (int g = 0; g < LG; g++) {
-            if (!lact[g]) continue;
+            const float* bp = g == 0 ? bp0 : bp1;
             if (MODE == 0) {
-              const float gv = B[base[g] + l * ein];
+              const float gv = bp[0];
               const float2 gg = make_float2(gv, gv);
-#pragma unroll
-              for (int j = 0; j < KG; j++) acc[g][j] = __ffma2_rn(gg, t1[j], acc[g][j]);
-            } else if (MODE == 1) {
-              const float xr = B[base[g] + l * ein], xi = B[base[g] + l * ein + 1];
-              const float2 rr = make_float2(xr, xr), ii = make_float2(xi, xi);
-#pragma unroll
-              for (int j = 0; j < KG; j++)
-                acc[g][j] = __ffma2_rn(ii, t2[j], __ffma2_rn(rr, t1[j], acc[g][j]));
+              ar[g][0] = __ffma2_rn(gg, tr01, ar[g][0]);
+              ar[g][1] = __ffma2_rn(gg, tr23, ar[g][1]);
+              ai[g][0] = __ffma2_rn(gg, ti01, ai[g][0]);
+              ai[g][1] = __ffma2_rn(gg, ti23, ai[g][1]);
             } else {
-              const float2 x = make_float2(B[base[g] + l * ein], B[base[g] + l * ein + 1]);
-#pragma unroll
-              for (int j = 0; j < KG; j++) acc[g][j] = __ffma2_rn(x, t1[j], acc[g][j]);
+              const float2 x = *reinterpret_cast<const float2*>(bp);
+              const float2 xr = make_float2(x.x, x.x), nxi = make_float2(-x.y, -x.y);
+              ar[g][0] = __ffma2_rn(nxi, ti01, __ffma2_rn(xr, tr01, ar[g][0]));
+              ar[g][1] = __ffma2_rn(nxi, ti23, __ffma2_rn(xr, tr23, ar[g][1]));
+              if (MODE == 1) {
+                const float2 xi = make_float2(x.y, x.y);
+                ai[g][0] = __ffma2_rn(xi, tr01, __ffma2_rn(xr, ti01, ai[g][0]));
+                ai[g][1] = __ffma2_rn(xi, tr23, __ffma2_rn(xr, ti23, ai[g][1]));
+              }
             }
           }
         }
@@ -136,14 +157,16 @@ __device__ __forceinline__ void pass_inplace(T* B, int nl, int nb, int SA, int S
       for (int g = 0; g < LG; g++) {
         if (!lact[g]) continue;
 #pragma unroll
-        for (int j = 0; j < KG; j++) {
-          const int k = kg + j * nkg;
+        for (int j = 0; j < 4; j++) {
+          const int k = 4 * kg + j;
           if (k >= nout) break;
+          const float re = (j & 1) ? ar[g][j >> 1].y : ar[g][j >> 1].x;
           if (MODE == 2) {
-            B[base[g] + k * eout] = acc[g][j].x + acc[g][j].y;
+            B[base[g] + k * eout] = re;
           } else {
-            B[base[g] + k * eout] = acc[g][j].x;
-            B[base[g] + k * eout + 1] = acc[g][j].y;
+            const float im = (j & 1) ? ai[g][j >> 1].y : ai[g][j >> 1].x;
+            B[base[g] + k * eout] = re;
+            B[base[g] + k * eout + 1] = im;
           }
         }
       }
@@ -151,6 +174,13 @@ __device__ __forceinline__ void pass_inplace(T* B, int nl, int nb, int SA, int S
     }
     return;
   }
+  // FP64: LG lines x KG outputs per thread, outputs interleaved over the lanes
+  constexpr int KG = 2;
+  const int nkg = (nout + KG - 1) / KG;
+  const int ngroups = blockDim.x / nkg;
+  const int t = threadIdx.x, lg = t / nkg, kg = t - lg * nkg;
+  const bool act_t = lg < ngroups;
+  const int lpr = ngroups * LG;
   for (int r0 = 0; r0 < nl; r0 += lpr) {
     T re[LG][KG], im[LG][KG];
     int base[LG];
@@ -170,8 +200,8 @@ __device__ __forceinline__ void pass_inplace(T* B, int nl, int nb, int SA, int S
         for (int j = 0; j < KG; j++) {
           const int k = kg + j * nkg;  // interleaved: neighbouring lanes, neighbouring modes
           const bool ok = k < nout;
-          tr[j] = ok ? tw[2 * (l * nout + k)] : T(0);
-          ti[j] = ok ? tw[2 * (l * nout + k) + 1] : T(0);
+          tr[j] = ok ? tw[(size_t)l * 2 * np + k] : T(0);
+          ti[j] = ok ? tw[(size_t)l * 2 * np + np + k] : T(0);
         }
 #pragma unroll
         for (int g = 0; g < LG; g++) {
@@ -887,6 +917,9 @@ void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s
   } else {
     S[0] = std::max(G, 2 * NH);
   }
+  // even last extent: every complex element (re, im) of the passes starts
+  // at an even element offset, as the FP32 passes' 8-byte loads require
+  S[P.dim - 1] += S[P.dim - 1] & 1;
   if (pad && sizeof(T) == 4 && P.dim >= 2) {
     int& last = S[P.dim - 1];
     while ((last - P.w) % 32 != 0 || (last & 1)) last++;
@@ -904,25 +937,28 @@ void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s
   a.beta = (T)P.beta;
   a.dscale = (T)(a.inv_dx_d * a.scale_d / a.hwdx_d);
   a.inv_sqd0 = (T)(1.0 / P.sqd0);
-  const size_t ntwf = 2 * (size_t)G * NF, ntwh = 2 * (size_t)G * NH, ntif = 2 * (size_t)NF * G,
-               ntih = 2 * (size_t)NH * G, total = ntwf + ntwh + ntif + ntih + 3 * (size_t)NF;
+  // planar rows: [l][re of nout padded | im of nout padded]
+  const int NFp = pad4(NF), NHp = pad4(NH), Gp = pad4(G);
+  const size_t ntwf = 2 * (size_t)G * NFp, ntwh = 2 * (size_t)G * NHp, ntif = 2 * (size_t)NF * Gp,
+               ntih = 2 * (size_t)NH * Gp, total = ntwf + ntwh + ntif + ntih + 3 * (size_t)NF;
   T* h = static_cast<T*>(pinned_stage(slot, sizeof(T) * total));
+  std::fill(h, h + total, T(0));
   T *twf = h, *twh = twf + ntwf, *tif = twh + ntwh, *tih = tif + ntif;
   T *facf = tih + ntih, *faci = facf + NF, *ts = faci + NF;
   for (int l = 0; l < G; l++) {
     double xl = (double)(P.l0 + l) * P.dx;
     for (int k = -K; k <= K; k++) {
       double c = cos(k * xl), sn = sin(k * xl);
-      twf[2 * (l * NF + k + K)] = (T)c;
-      twf[2 * (l * NF + k + K) + 1] = (T)(-sn);
-      tif[2 * ((k + K) * G + l)] = (T)c;
-      tif[2 * ((k + K) * G + l) + 1] = (T)sn;
+      twf[(size_t)l * 2 * NFp + k + K] = (T)c;
+      twf[(size_t)l * 2 * NFp + NFp + k + K] = (T)(-sn);
+      tif[(size_t)(k + K) * 2 * Gp + l] = (T)c;
+      tif[(size_t)(k + K) * 2 * Gp + Gp + l] = (T)sn;
       if (k >= 0) {
-        twh[2 * (l * NH + k)] = (T)c;
-        twh[2 * (l * NH + k) + 1] = (T)(-sn);
+        twh[(size_t)l * 2 * NHp + k] = (T)c;
+        twh[(size_t)l * 2 * NHp + NHp + k] = (T)(-sn);
         double f = k == 0 ? 1.0 : 2.0;
-        tih[2 * (k * G + l)] = (T)(f * c);
-        tih[2 * (k * G + l) + 1] = (T)(f * sn);
+        tih[(size_t)k * 2 * Gp + l] = (T)(f * c);
+        tih[(size_t)k * 2 * Gp + Gp + l] = (T)(f * sn);
       }
     }
   }

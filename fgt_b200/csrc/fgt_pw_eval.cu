@@ -68,7 +68,7 @@ __device__ __forceinline__ void build_eval_grid(const PWArgs<T>& a, const T* L, 
         const T f = a.faci[k + K];
         const T lr = L[2 * k] * f, li = L[2 * k + 1] * f;
         const T mr = lr * fr - li * fi, mi = lr * fi + li * fr;
-        acc += mr * tih[2 * (k * G + l)] - mi * tih[2 * (k * G + l) + 1];
+        acc += mr * tih[k * 2 * pad4(G) + l] - mi * tih[k * 2 * pad4(G) + pad4(G) + l];
       }
       B[l] = acc;
     }
@@ -136,9 +136,10 @@ __global__ void __launch_bounds__(eval_threads<T, DIM, W, GB, DERIV>())
   const Geo& g = a.g;
   const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
   T* sm = reinterpret_cast<T*>(smem_raw);
-  T* tif = sm;
-  T* tih = tif + 2 * NF * G;
-  int* ordtmp = reinterpret_cast<int*>(tih + 2 * NH * G);
+  const int Gp = pad4(G);
+  T* tif = sm;                 // planar rows of 2*Gp
+  T* tih = tif + 2 * NF * Gp;
+  int* ordtmp = reinterpret_cast<int*>(sm + tw_elems(G, K));
   int* ordcnt = ordtmp + ORDER_CHUNK;
   unsigned short* perm = reinterpret_cast<unsigned short*>(ordcnt + 32);
   int* bins = reinterpret_cast<int*>(smem_raw + order_offset<T>(G, K));  // NBINS_MAX
@@ -150,8 +151,8 @@ __global__ void __launch_bounds__(eval_threads<T, DIM, W, GB, DERIV>())
     if constexpr (GB) return static_cast<const T*>(B);
     else return SmemView<T>{(int)(eval_offset<T>(G, K) / sizeof(T))};
   }();
-  load_tw(tif, a.tif, 2 * NF * G);
-  load_tw(tih, a.tih, 2 * NH * G);
+  load_tw(tif, a.tif, 2 * NF * Gp);
+  load_tw(tih, a.tih, 2 * NH * Gp);
   __syncthreads();
   // shared-space byte address of the grid (shared-memory grid variants)
   const uint32_t grid_saddr =
