@@ -281,10 +281,13 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
         if (DIM == 3) {
           pass_inplace<T, 0>(B, G * G, G, g.str[0], g.str[1], 1, 2, G, NH, twh);
           pass_inplace<T, 1>(B, G * NH, NH, g.str[0], 2, g.str[1], g.str[1], G, NF, twf);
+          pass_inplace<T, 1>(B, NF * NH, NH, g.str[1], 2, g.str[0], g.str[0], G, NF, twf);
         } else if (DIM == 2) {
           pass_inplace<T, 0>(B, G, 1, g.str[0], 0, 1, 2, G, NH, twh);
+          pass_inplace<T, 1>(B, NH, 1, 2, 0, g.str[0], g.str[0], G, NF, twf);
         }
-        // final pass along x to the expansion, with weights and deconvolution
+        // expansion: the x pass's modes (1D: the pass along x here) with
+        // weights and deconvolution
         const int nline = DIM == 3 ? NF * NH : (DIM == 2 ? NH : 1);
         const int nko = DIM == 1 ? NH : NF;
         for (int o = threadIdx.x; o < nko * nline; o += blockDim.x) {
@@ -308,12 +311,8 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
               im += gv * twh[l * 2 * NHp + NHp + kxi];
             }
           } else {
-            for (int l = 0; l < G; l++) {
-              const T xr = B[l * g.str[0] + lb], xi = B[l * g.str[0] + lb + 1];
-              const T tr = twf[l * 2 * NFp + kxi], ti = twf[l * 2 * NFp + NFp + kxi];
-              re += xr * tr - xi * ti;
-              im += xr * ti + xi * tr;
-            }
+            re = B[kxi * g.str[0] + lb];
+            im = B[kxi * g.str[0] + lb + 1];
           }
           int ki[3];
           if (DIM == 3) { ki[0] = kxi; ki[1] = kyi; ki[2] = kz + K; }
