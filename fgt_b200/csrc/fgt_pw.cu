@@ -345,6 +345,7 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
 }
 
 // ---------------------------------------------------------------- translate
+constexpr int TRANS_MPT = 4;
 // Local expansion of every eval box: its own form expansion plus the
 // diagonal translations W[w] * M[s] of its list (gnd_shiftpw,
 // src/pfgt/bfgt_pwrouts.f:1555-1636), one mode per thread, complex values
@@ -355,26 +356,49 @@ __global__ void k_translate(int n_eval, int nexp, int nd, int ge, const int* __r
                             const int* __restrict__ widx, const T* __restrict__ mp,
                             const T* __restrict__ wtab, T* __restrict__ loc) {
   using V = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+  constexpr int MPT = TRANS_MPT;  // modes per thread, blockDim apart
   const V* mpv = reinterpret_cast<const V*>(mp);
   const V* wv = reinterpret_cast<const V*>(wtab);
   V* lv = reinterpret_cast<V*>(loc);
   const int e0 = blockIdx.y * ge, e1 = min(n_eval, e0 + ge);
-  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < nexp; m += gridDim.x * blockDim.x) {
-    for (int e = e0; e < e1; e++) {
-      const int sf = self[e], j0 = ptr[e], j1 = ptr[e + 1];
-      for (int id = 0; id < nd; id++) {
-        V acc;
-        acc.x = T(0);
-        acc.y = T(0);
-        if (sf >= 0) acc = __ldg(mpv + ((size_t)sf * nd + id) * nexp + m);
-        for (int j = j0; j < j1; j++) {
-          const V av = __ldg(mpv + ((size_t)src[j] * nd + id) * nexp + m);
-          const V w = __ldg(wv + (size_t)widx[j] * nexp + m);
-          acc.x += av.x * w.x - av.y * w.y;
-          acc.y += av.x * w.y + av.y * w.x;
-        }
-        lv[((size_t)e * nd + id) * nexp + m] = acc;
+  const int m0 = blockIdx.x * blockDim.x * MPT + threadIdx.x;
+  bool ok[MPT];
+#pragma unroll
+  for (int i = 0; i < MPT; i++) ok[i] = m0 + i * (int)blockDim.x < nexp;
+  for (int e = e0; e < e1; e++) {
+    const int sf = self[e], j0 = ptr[e], j1 = ptr[e + 1];
+    for (int id = 0; id < nd; id++) {
+      V acc[MPT];
+      const V* sp = mpv + ((size_t)(sf >= 0 ? sf : 0) * nd + id) * nexp + m0;
+#pragma unroll
+      for (int i = 0; i < MPT; i++) {
+        acc[i].x = T(0);
+        acc[i].y = T(0);
+        if (sf >= 0 && ok[i]) acc[i] = __ldg(sp + i * blockDim.x);
       }
+      for (int j = j0; j < j1; j++) {
+        const V* ap = mpv + ((size_t)src[j] * nd + id) * nexp + m0;
+        const V* wp = wv + (size_t)widx[j] * nexp + m0;
+        V av[MPT], w[MPT];
+#pragma unroll
+        for (int i = 0; i < MPT; i++) {
+          if (ok[i]) {
+            av[i] = __ldg(ap + i * blockDim.x);
+            w[i] = __ldg(wp + i * blockDim.x);
+          } else {
+            av[i].x = av[i].y = w[i].x = w[i].y = T(0);
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < MPT; i++) {
+          acc[i].x += av[i].x * w[i].x - av[i].y * w[i].y;
+          acc[i].y += av[i].x * w[i].y + av[i].y * w[i].x;
+        }
+      }
+      V* op = lv + ((size_t)e * nd + id) * nexp + m0;
+#pragma unroll
+      for (int i = 0; i < MPT; i++)
+        if (ok[i]) op[i * blockDim.x] = acc[i];
     }
   }
 }
@@ -662,10 +686,10 @@ int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, PWWork* work, 
     work->bytes_translate = (double)sizeof(T) * 2 * P.nexp * P.nd *
                             ((double)L.n_trans + 2.0 * L.n_eval);
   if (L.n_eval == 0) return 1;
-  // a thread runs one mode of TGE consecutive eval boxes, which share most
-  // of their source expansions: the repeated reads hit L1
+  // a thread runs TRANS_MPT modes of TGE consecutive eval boxes, which
+  // share most of their source expansions: the repeated reads hit L1
   constexpr int TGE = 4;
-  int gx = std::max(1, std::min(ceil_div(P.nexp, 256), 64));
+  int gx = std::max(1, ceil_div(P.nexp, 256 * TRANS_MPT));
   for (int e0 = 0; e0 < L.n_eval; e0 += 65535 * TGE) {
     int ne = std::min(65535 * TGE, L.n_eval - e0);
     dim3 grid(gx, ceil_div(ne, TGE));
