@@ -27,16 +27,51 @@ namespace fgt {
 
 namespace {
 
-template <typename T>
-__global__ void k_gather_coords(const double* __restrict__ x, int n, int dim,
+// Point gathers run UB points per thread per round (rounds a grid stride
+// apart) with all their index and data loads issued before the stores: the
+// random reads are latency bound, so the independent loads overlap.
+constexpr int UB = 4;
+
+template <typename T, int DIM>
+__global__ void k_gather_coords(const double* __restrict__ x, int n,
                                 const uint32_t* __restrict__ perm, const int* __restrict__ ref,
                                 const double* __restrict__ center, T* __restrict__ off) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    size_t o = perm[i];
-    int b = ref[i];
-    for (int k = 0; k < dim; k++)
-      off[(size_t)k * n + i] = (T)(x[o * dim + k] - center[(size_t)b * dim + k]);
+  const int st = gridDim.x * blockDim.x;
+  for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += UB * st) {
+    size_t o[UB];
+    int b[UB];
+#pragma unroll
+    for (int u = 0; u < UB; u++) {
+      const int i = i0 + u * st;
+      o[u] = i < n ? perm[i] : 0;
+      b[u] = i < n ? ref[i] : 0;
+    }
+    double v[UB][DIM], c[UB][DIM];
+#pragma unroll
+    for (int u = 0; u < UB; u++)
+#pragma unroll
+      for (int k = 0; k < DIM; k++) {
+        const bool in = i0 + u * st < n;
+        v[u][k] = in ? x[o[u] * DIM + k] : 0.0;
+        c[u][k] = in ? center[(size_t)b[u] * DIM + k] : 0.0;
+      }
+#pragma unroll
+    for (int u = 0; u < UB; u++) {
+      const int i = i0 + u * st;
+      if (i < n)
+#pragma unroll
+        for (int k = 0; k < DIM; k++) off[(size_t)k * n + i] = (T)(v[u][k] - c[u][k]);
+    }
   }
+}
+template <typename T>
+void launch_gather_coords(int dim, const double* x, int n, const uint32_t* perm, const int* ref,
+                          const double* center, T* off, cudaStream_t s) {
+  const int grid = grid_for(n, 256);
+  if (dim == 1) k_gather_coords<T, 1><<<grid, 256, 0, s>>>(x, n, perm, ref, center, off);
+  else if (dim == 2) k_gather_coords<T, 2><<<grid, 256, 0, s>>>(x, n, perm, ref, center, off);
+  else k_gather_coords<T, 3><<<grid, 256, 0, s>>>(x, n, perm, ref, center, off);
+  FGT_LAUNCH_CHECK();
 }
 
 template <typename T>
@@ -62,16 +97,36 @@ __global__ void k_gather_out(const double* __restrict__ srt, int n, int nd, int 
                              const uint32_t* __restrict__ inv, double* __restrict__ pot,
                              double* __restrict__ grad, double* __restrict__ hess) {
   const int nh = dim * (dim + 1) / 2;
-  for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n; o += gridDim.x * blockDim.x) {
-    const size_t i = inv[o];
+  const int st = gridDim.x * blockDim.x;
+  for (int o0 = blockIdx.x * blockDim.x + threadIdx.x; o0 < n; o0 += UB * st) {
+    size_t iu[UB];
+#pragma unroll
+    for (int u = 0; u < UB; u++) iu[u] = o0 + u * st < n ? inv[o0 + u * st] : 0;
     for (int id = 0; id < nd; id++) {
-      pot[(size_t)o * nd + id] = srt[(size_t)id * n + i];
+      double v[UB];
+#pragma unroll
+      for (int u = 0; u < UB; u++) v[u] = o0 + u * st < n ? srt[(size_t)id * n + iu[u]] : 0.0;
+#pragma unroll
+      for (int u = 0; u < UB; u++)
+        if (o0 + u * st < n) pot[(size_t)(o0 + u * st) * nd + id] = v[u];
       if (pgh >= 2)
-        for (int k = 0; k < dim; k++)
-          grad[((size_t)o * dim + k) * nd + id] = srt[((size_t)(1 + k) * nd + id) * n + i];
+        for (int k = 0; k < dim; k++) {
+#pragma unroll
+          for (int u = 0; u < UB; u++)
+            v[u] = o0 + u * st < n ? srt[((size_t)(1 + k) * nd + id) * n + iu[u]] : 0.0;
+#pragma unroll
+          for (int u = 0; u < UB; u++)
+            if (o0 + u * st < n) grad[((size_t)(o0 + u * st) * dim + k) * nd + id] = v[u];
+        }
       if (pgh >= 3)
-        for (int m = 0; m < nh; m++)
-          hess[((size_t)o * nh + m) * nd + id] = srt[((size_t)(1 + dim + m) * nd + id) * n + i];
+        for (int m = 0; m < nh; m++) {
+#pragma unroll
+          for (int u = 0; u < UB; u++)
+            v[u] = o0 + u * st < n ? srt[((size_t)(1 + dim + m) * nd + id) * n + iu[u]] : 0.0;
+#pragma unroll
+          for (int u = 0; u < UB; u++)
+            if (o0 + u * st < n) hess[((size_t)(o0 + u * st) * nh + m) * nd + id] = v[u];
+        }
     }
   }
 }
@@ -261,14 +316,10 @@ void setup_geometry(Setup& u, const Call& c, double* bs0_io, double* cen0_io, co
   // --- gather (dreorderf, fmmcommon2d.f:3-27) as offsets from reference boxes
   u.soff.alloc((size_t)c.ns * dim, s);
   u.toff.alloc((size_t)std::max(c.nt, 1) * dim, s);
-  k_gather_coords<double><<<grid_for(c.ns, 256), 256, 0, s>>>(c.src, c.ns, dim, t.isrc, t.src_ref,
-                                                              t.center, u.soff);
-  FGT_LAUNCH_CHECK();
+  launch_gather_coords<double>(dim, c.src, c.ns, t.isrc, t.src_ref, t.center, u.soff, s);
   launches++;
   if (c.nt > 0) {
-    k_gather_coords<double><<<grid_for(c.nt, 256), 256, 0, s>>>(c.trg, c.nt, dim, t.itrg,
-                                                                t.trg_ref, t.center, u.toff);
-    FGT_LAUNCH_CHECK();
+    launch_gather_coords<double>(dim, c.trg, c.nt, t.itrg, t.trg_ref, t.center, u.toff, s);
     launches++;
   }
   // inverse leaf permutations for the output reorder
