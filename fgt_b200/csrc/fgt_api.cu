@@ -221,8 +221,18 @@ struct Setup {
 };
 
 // Records of the packed list-1 sources are 64 bytes; above this count (4 GiB)
-// the near field walks the list instead.
+// the near field walks the list instead.  FGT_NEAR_PACK_MAX (a record count,
+// 0 = never pack) lowers the cap, e.g. to test the list-walking kernel.
 constexpr long long kMaxNearRecords = 1ll << 26;
+long long near_pack_max() {
+  const char* e = getenv("FGT_NEAR_PACK_MAX");
+  if (e && *e) {
+    char* end = nullptr;
+    const long long v = strtoll(e, &end, 10);
+    if (end != e && v >= 0) return std::min(v, kMaxNearRecords);
+  }
+  return kMaxNearRecords;
+}
 
 DirectGeom direct_geom(const Setup& u) {
   DirectGeom g;
@@ -337,7 +347,7 @@ void setup_geometry(Setup& u, const Call& c, double* bs0_io, double* cen0_io, co
   u.iperiod0 = iperiod0;
   if (near_lists && u.L.n_l1 > 0) {
     u.near_total = near_lists_count(direct_geom(u), u.L, t.src_lo, t.src_hi, t.trg_lo, t.trg_hi,
-                                    u.soff, c.ns, kMaxNearRecords, u.near_pos, s);
+                                    u.soff, c.ns, near_pack_max(), u.near_pos, s);
     launches += 2;
   }
   u.ndiv = ndiv;
