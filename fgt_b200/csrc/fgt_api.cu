@@ -159,6 +159,31 @@ cudaStream_t library_stream(int dev) {
   return streams[dev];
 }
 
+// Per-thread side stream for the strength copies of host-buffer calls, and
+// its two events (copy may start, copy done).
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t gate = nullptr, done = nullptr;
+};
+SideStream& side_stream(int dev) {
+  static thread_local SideStream ss[64];
+  SideStream& x = ss[dev < 0 || dev >= 64 ? 0 : dev];
+  if (!x.s) {
+    FGT_CUDA(cudaStreamCreateWithFlags(&x.s, cudaStreamNonBlocking));
+    FGT_CUDA(cudaEventCreateWithFlags(&x.gate, cudaEventDisableTiming));
+    FGT_CUDA(cudaEventCreateWithFlags(&x.done, cudaEventDisableTiming));
+  }
+  return x;
+}
+// Waits for the side stream when a call leaves (also on error paths), so
+// no copy into the call's workspace outlives it.
+struct SideSync {
+  cudaStream_t s = nullptr;
+  ~SideSync() {
+    if (s) (void)cudaStreamSynchronize(s);
+  }
+};
+
 struct Timer {
   bool on;
   cudaStream_t s;
@@ -197,6 +222,9 @@ struct Call {
   double delta, eps;
   const double *src, *q, *rn, *ds, *trg;  // device pointers
   double *pot, *grad, *hess, *pott, *gradt, *hesst;  // device pointers
+  // host-buffer calls: q/rn/ds arrive on a side stream while the tree is
+  // built; the strength-dependent part waits for this event
+  cudaEvent_t strengths_ready = nullptr;
 };
 
 // Point-dependent part of a call: scalar set-up, tree, lists, sorted FP64
@@ -368,6 +396,7 @@ void execute(const Setup& u, const Call& c, const fgt_opts& o, fgt_stats* st, cu
   const Tree& t = u.t;
   const Lists& L = u.L;
   int launches = u.launches;
+  if (c.strengths_ready) FGT_CUDA(cudaStreamWaitEvent(s, c.strengths_ready, 0));
   DBuf<T> qs, dss, rns;
   if (c.ifcharge) {
     qs.alloc((size_t)c.ns * nd, s);
@@ -577,10 +606,30 @@ int pfgt_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps
     return b.get();
   };
   c.src = h2d(d_src, sources, (size_t)ns * dim);
-  c.q = c.ifcharge ? h2d(d_q, charge, (size_t)ns * nd) : nullptr;
-  c.rn = c.ifdipole ? h2d(d_rn, rnormal, (size_t)ns * dim) : nullptr;
-  c.ds = c.ifdipole ? h2d(d_ds, dipstr, (size_t)ns * nd) : nullptr;
   c.trg = nt > 0 ? h2d(d_trg, targ, (size_t)nt * dim) : c.src;
+  SideSync side_sync;
+  if (o.device_ptrs) {
+    c.q = c.ifcharge ? charge : nullptr;
+    c.rn = c.ifdipole ? rnormal : nullptr;
+    c.ds = c.ifdipole ? dipstr : nullptr;
+  } else {
+    // strengths are first needed after the tree and lists: copy them on the
+    // side stream meanwhile
+    SideStream& ss = side_stream(dev);
+    auto side = [&](DBuf<double>& b, const double* h, size_t n) -> const double* {
+      b.alloc(n, s);
+      FGT_CUDA(cudaMemcpyAsync(b.get(), h, sizeof(double) * n, cudaMemcpyHostToDevice, ss.s));
+      return b.get();
+    };
+    FGT_CUDA(cudaEventRecord(ss.gate, s));
+    FGT_CUDA(cudaStreamWaitEvent(ss.s, ss.gate, 0));
+    side_sync.s = ss.s;
+    c.q = c.ifcharge ? side(d_q, charge, (size_t)ns * nd) : nullptr;
+    c.rn = c.ifdipole ? side(d_rn, rnormal, (size_t)ns * dim) : nullptr;
+    c.ds = c.ifdipole ? side(d_ds, dipstr, (size_t)ns * nd) : nullptr;
+    FGT_CUDA(cudaEventRecord(ss.done, ss.s));
+    c.strengths_ready = ss.done;
+  }
   c.pot = ifpgh >= 1 ? dout(d_pot, pot, (size_t)ns * nd) : nullptr;
   c.grad = ifpgh >= 2 ? dout(d_grad, grad, (size_t)ns * nd * dim) : nullptr;
   c.hess = ifpgh >= 3 ? dout(d_hess, hess, (size_t)ns * nd * nhess) : nullptr;
