@@ -163,7 +163,7 @@ cudaStream_t library_stream(int dev) {
 // its two events (copy may start, copy done).
 struct SideStream {
   cudaStream_t s = nullptr;
-  cudaEvent_t gate = nullptr, done = nullptr;
+  cudaEvent_t gate = nullptr, done = nullptr, out = nullptr;
 };
 SideStream& side_stream(int dev) {
   static thread_local SideStream ss[64];
@@ -172,6 +172,7 @@ SideStream& side_stream(int dev) {
     FGT_CUDA(cudaStreamCreateWithFlags(&x.s, cudaStreamNonBlocking));
     FGT_CUDA(cudaEventCreateWithFlags(&x.gate, cudaEventDisableTiming));
     FGT_CUDA(cudaEventCreateWithFlags(&x.done, cudaEventDisableTiming));
+    FGT_CUDA(cudaEventCreateWithFlags(&x.out, cudaEventDisableTiming));
   }
   return x;
 }
@@ -225,6 +226,10 @@ struct Call {
   // host-buffer calls: q/rn/ds arrive on a side stream while the tree is
   // built; the strength-dependent part waits for this event
   cudaEvent_t strengths_ready = nullptr;
+  // when set: the source outputs are finished (near field and reorder of
+  // the sources before those of the targets) when this event completes, so
+  // their device-to-host copy overlaps the targets' remaining work
+  cudaEvent_t sources_done = nullptr;
 };
 
 // Point-dependent part of a call: scalar set-up, tree, lists, sorted FP64
@@ -469,11 +474,24 @@ void execute(const Setup& u, const Call& c, const fgt_opts& o, fgt_stats* st, cu
       packed.rec = near_rec;
     }
   }
-  launches += direct_near_field<T>(g, L, src, et, st ? &pairs : nullptr, s, &packed);
-  launches += direct_near_field<T>(g, L, src, es, st ? &pairs : nullptr, s, &packed);
+  if (c.sources_done) {
+    // sources first, then signal; the targets follow
+    launches += direct_near_field<T>(g, L, src, es, st ? &pairs : nullptr, s, &packed);
+    if (c.ifpgh >= 1) {
+      k_gather_out<<<grid_for(c.ns, 256), 256, 0, s>>>(outs, c.ns, nd, dim, c.ifpgh, u.inv_s,
+                                                       c.pot, c.grad, c.hess);
+      FGT_LAUNCH_CHECK();
+      launches++;
+    }
+    FGT_CUDA(cudaEventRecord(c.sources_done, s));
+    launches += direct_near_field<T>(g, L, src, et, st ? &pairs : nullptr, s, &packed);
+  } else {
+    launches += direct_near_field<T>(g, L, src, et, st ? &pairs : nullptr, s, &packed);
+    launches += direct_near_field<T>(g, L, src, es, st ? &pairs : nullptr, s, &packed);
+  }
   tm.mark(7);
   // --- back to input order
-  if (c.ifpgh >= 1) {
+  if (c.ifpgh >= 1 && !c.sources_done) {
     k_gather_out<<<grid_for(c.ns, 256), 256, 0, s>>>(outs, c.ns, nd, dim, c.ifpgh, u.inv_s, c.pot,
                                                      c.grad, c.hess);
     FGT_LAUNCH_CHECK();
@@ -608,6 +626,7 @@ int pfgt_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps
   c.src = h2d(d_src, sources, (size_t)ns * dim);
   c.trg = nt > 0 ? h2d(d_trg, targ, (size_t)nt * dim) : c.src;
   SideSync side_sync;
+  SideStream* ssp = nullptr;
   if (o.device_ptrs) {
     c.q = c.ifcharge ? charge : nullptr;
     c.rn = c.ifdipole ? rnormal : nullptr;
@@ -616,6 +635,7 @@ int pfgt_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps
     // strengths are first needed after the tree and lists: copy them on the
     // side stream meanwhile
     SideStream& ss = side_stream(dev);
+    ssp = &ss;
     auto side = [&](DBuf<double>& b, const double* h, size_t n) -> const double* {
       b.alloc(n, s);
       FGT_CUDA(cudaMemcpyAsync(b.get(), h, sizeof(double) * n, cudaMemcpyHostToDevice, ss.s));
@@ -629,6 +649,7 @@ int pfgt_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps
     c.ds = c.ifdipole ? side(d_ds, dipstr, (size_t)ns * nd) : nullptr;
     FGT_CUDA(cudaEventRecord(ss.done, ss.s));
     c.strengths_ready = ss.done;
+    c.sources_done = ss.out;
   }
   c.pot = ifpgh >= 1 ? dout(d_pot, pot, (size_t)ns * nd) : nullptr;
   c.grad = ifpgh >= 2 ? dout(d_grad, grad, (size_t)ns * nd * dim) : nullptr;
@@ -640,15 +661,23 @@ int pfgt_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps
   if (prec == FGT_PREC_FP64) run_pfgt<double>(c, bs0, cen0, o, st, s, tm);
   else run_pfgt<float>(c, bs0, cen0, o, st, s, tm);
   if (!o.device_ptrs) {
-    auto d2h = [&](double* h, const DBuf<double>& b, size_t n) {
-      if (h && b.p) FGT_CUDA(cudaMemcpyAsync(h, b.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    // source outputs on the side stream once they are final, target outputs
+    // on the call's stream
+    cudaStream_t so = side_sync.s ? side_sync.s : s;
+    if (side_sync.s && c.sources_done) FGT_CUDA(cudaStreamWaitEvent(so, c.sources_done, 0));
+    auto d2h = [&](double* h, const DBuf<double>& b, size_t n, cudaStream_t q) {
+      if (h && b.p) FGT_CUDA(cudaMemcpyAsync(h, b.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, q));
     };
-    if (ifpgh >= 1) d2h(pot, d_pot, (size_t)ns * nd);
-    if (ifpgh >= 2) d2h(grad, d_grad, (size_t)ns * nd * dim);
-    if (ifpgh >= 3) d2h(hess, d_hess, (size_t)ns * nd * nhess);
-    if (c.ifpghtarg >= 1) d2h(pottarg, d_pt, (size_t)nt * nd);
-    if (c.ifpghtarg >= 2) d2h(gradtarg, d_gt, (size_t)nt * nd * dim);
-    if (c.ifpghtarg >= 3) d2h(hesstarg, d_ht, (size_t)nt * nd * nhess);
+    if (ifpgh >= 1) d2h(pot, d_pot, (size_t)ns * nd, so);
+    if (ifpgh >= 2) d2h(grad, d_grad, (size_t)ns * nd * dim, so);
+    if (ifpgh >= 3) d2h(hess, d_hess, (size_t)ns * nd * nhess, so);
+    if (c.ifpghtarg >= 1) d2h(pottarg, d_pt, (size_t)nt * nd, s);
+    if (c.ifpghtarg >= 2) d2h(gradtarg, d_gt, (size_t)nt * nd * dim, s);
+    if (c.ifpghtarg >= 3) d2h(hesstarg, d_ht, (size_t)nt * nd * nhess, s);
+    if (so != s && ssp) {  // the call's stream completes after the side copies
+      FGT_CUDA(cudaEventRecord(ssp->gate, so));
+      FGT_CUDA(cudaStreamWaitEvent(s, ssp->gate, 0));
+    }
   }
   tm.mark(9);
   FGT_CUDA(cudaStreamSynchronize(s));
