@@ -45,6 +45,11 @@ def parse():
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--profile-once", action="store_true",
                    help="one untimed step only (for ncu launch lists)")
+    p.add_argument("--sweep", default="none", choices=["none", "cells", "all"],
+                   help="also time the benchmark's other configurations: 'cells' = the "
+                        "delta/eps cells of the sphere workload at eps=1e-6 plus configs 1-3, "
+                        "'all' = every delta x eps cell")
+    p.add_argument("--sweep-only", action="store_true", help="skip the headline extras")
     return p.parse_args()
 
 
@@ -206,6 +211,203 @@ def cpu_reference(cfg, target_s=10.0, frac=None):
     return npts / t, desc, O.threads(), frac
 
 
+def _ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+def exact_sample(F, dev, stream, cfg, pts_d, pgh):
+    """FP64 direct sum over all sources (no cut-off; periodic: images
+    |n_d| <= 1, enough for delta <= 1e-3 on the unit cell) at pts_d, by the
+    library's all-pairs kernel."""
+    import ctypes as C
+    import itertools
+    import torch
+    n, nd, dim = pts_d.shape[0], cfg["nd"], cfg["dim"]
+    ep = torch.zeros((n, nd), dtype=torch.float64, device=dev)
+    eg = torch.zeros((n, dim, nd), dtype=torch.float64, device=dev)
+    L = F.lib()
+    f = L.fgt_direct_nomalloc
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_int,
+                  C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                  C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                  C.c_void_p]
+    src_d = cfg["_src_d"]
+    q_d = cfg["_q_d"]
+    shifts = [None]
+    if cfg["iperiod"] == 1:
+        shifts = [np.array(v, dtype=np.float64) * cfg["bs0"]
+                  for v in itertools.product((-1.0, 0.0, 1.0), repeat=dim)]
+    for sh in shifts:
+        rc = f(nd, dim, cfg["delta"], 1e300,
+               None if sh is None else sh.ctypes.data_as(C.c_void_p), src_d.shape[0],
+               src_d.data_ptr(), 1, q_d.data_ptr(), 0, None, None, n, pts_d.data_ptr(), pgh,
+               ep.data_ptr(), eg.data_ptr() if pgh >= 2 else None, None,
+               C.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError("fgt_direct_nomalloc failed: %d" % rc)
+    torch.cuda.synchronize()
+    return ep, eg
+
+
+def run_cell(F, dev, stream, cfg, prec, steps, warmup, exact=None):
+    """Time one configuration at one precision (device-resident inputs and
+    outputs, CUDA events on the launching stream) and measure its relative
+    l2 error at a sample of 1000 + 1000 points against the FP64 direct sum."""
+    import ctypes as C
+    import torch
+    nd, dim = cfg["nd"], cfg["dim"]
+    N = cfg["sources"].shape[0]
+    has_t = cfg.get("targets") is not None
+    M = cfg["targets"].shape[0] if has_t else 0
+    if "_src_d" not in cfg:
+        cfg["_src_d"] = torch.from_numpy(cfg["sources"]).to(dev)
+        cfg["_q_d"] = torch.from_numpy(np.ascontiguousarray(cfg["charge"])).to(dev)
+        cfg["_trg_d"] = torch.from_numpy(cfg["targets"]).to(dev) if has_t else None
+    src_d, q_d, trg_d = cfg["_src_d"], cfg["_q_d"], cfg["_trg_d"]
+    pgh, pght = cfg["ifpgh"], cfg["ifpghtarg"] if has_t else 0
+    pot = torch.empty((N, nd), dtype=torch.float64, device=dev)
+    grad = torch.empty((N, dim, nd), dtype=torch.float64, device=dev) if pgh >= 2 else None
+    pt = torch.empty((max(M, 1), nd), dtype=torch.float64, device=dev)
+    gt = torch.empty((max(M, 1), dim, nd), dtype=torch.float64, device=dev) if pght >= 2 else None
+    st = F.FgtStats()
+    o = F.FgtOpts()
+    F.lib().fgt_opts_default(C.byref(o))
+    o.precision = prec
+    o.device_ptrs = 1
+    o.device = dev.index
+    o.stream = C.c_void_p(stream.cuda_stream)
+    b0 = cfg.get("bs0", 1.0)
+    c0 = cfg.get("cen0", [0.0] * 3)
+
+    def step(opts):
+        F.pfgt_device(opts, nd, dim, cfg["delta"], cfg["eps"], cfg["iperiod"], b0, c0, N,
+                      src_d.data_ptr(), 1, q_d.data_ptr(), 0, None, None, pgh, pot.data_ptr(),
+                      _ptr(grad), None, M, _ptr(trg_d), pght, pt.data_ptr() if M else None,
+                      _ptr(gt), None)
+
+    for _ in range(warmup):
+        step(o)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step(o)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    ot = F.FgtOpts()
+    F.lib().fgt_opts_default(C.byref(ot))
+    ot.precision, ot.device_ptrs, ot.device = prec, 1, dev.index
+    ot.stream = C.c_void_p(stream.cuda_stream)
+    ot.timing = 1
+    ot.stats = C.pointer(st)
+    step(ot)
+    torch.cuda.synchronize()
+    sd = st.as_dict()
+    npts = N * (pgh > 0) + M * (pght > 0)
+    out = {"precision": "fp64" if prec == F.PREC_FP64 else "mixed", "ms": ms,
+           "value": npts / (ms * 1e-3), "unit": "pts/s", "steps": steps,
+           "phases_ms": {k: round(float(v), 3) for k, v in zip(
+               ["h2d", "tree", "sort_gather", "lists", "form", "translate", "eval", "direct",
+                "scatter", "d2h", "total"], sd["ms"][:11])},
+           "stats": {k: sd[k] for k in ("npwlevel", "nlevels", "npw", "n_form_boxes",
+                                         "n_eval_boxes", "near_pairs", "spread_width")}}
+    if exact is not None:
+        i_s, x_sp, x_sg, i_t, x_tp, x_tg = exact
+        rp = [(x_sp, pot[i_s])]
+        rg = [(x_sg, grad[i_s])] if pgh >= 2 else []
+        if M and pght >= 1:
+            rp.append((x_tp, pt[i_t]))
+            if pght >= 2:
+                rg.append((x_tg, gt[i_t]))
+
+        def rel(pairs):
+            ref = torch.cat([r.reshape(-1) for r, _ in pairs])
+            got = torch.cat([g.reshape(-1) for _, g in pairs])
+            return float(torch.linalg.norm(ref - got) / torch.linalg.norm(ref))
+
+        out["rel_l2"] = {"pot": rel(rp)}
+        if rg:
+            out["rel_l2"]["grad"] = rel(rg)
+    out["_outputs"] = (pot, grad, pt if M else None, gt)
+    return out
+
+
+def exact_for(F, dev, stream, cfg, nsample=1000):
+    import torch
+    g = torch.Generator().manual_seed(7)
+    N = cfg["sources"].shape[0]
+    has_t = cfg.get("targets") is not None
+    M = cfg["targets"].shape[0] if has_t else 0
+    pgh = max(cfg["ifpgh"], cfg["ifpghtarg"] if has_t else 0)
+    i_s = torch.randperm(N, generator=g)[:min(nsample, N)].to(dev)
+    xs_p, xs_g = exact_sample(F, dev, stream, cfg, cfg["_src_d"][i_s].contiguous(), pgh)
+    i_t, xt_p, xt_g = None, None, None
+    if M:
+        i_t = torch.randperm(M, generator=g)[:min(nsample, M)].to(dev)
+        xt_p, xt_g = exact_sample(F, dev, stream, cfg, cfg["_trg_d"][i_t].contiguous(), pgh)
+    return i_s, xs_p, xs_g, i_t, xt_p, xt_g
+
+
+def sweep(a, F, dev, stream, W):
+    """The benchmark's configurations besides the headline, each with the
+    mixed path (where eps >= 1e-6, and for configuration 2 by its own
+    definition) and the FP64 path side by side."""
+    import torch
+    cells = []
+    plan = [("config1", W.config(1), None), ("config2", W.config(2), None),
+            ("config3", W.config(3), None)]
+    c5 = W.config(5)
+    deltas = (1e-6, 1e-4, 1e-2, 1e-1)
+    epss = (1e-3, 1e-6, 1e-9, 1e-12) if a.sweep == "all" else (1e-6,)
+    for d in deltas:
+        for e in epss:
+            cfg = dict(c5)
+            cfg["delta"], cfg["eps"] = d, e
+            plan.append(("config5 delta=%g eps=%g" % (d, e), cfg, d))
+    exact_cache = {}
+    for name, cfg, dkey in plan:
+        cfg = {k: v for k, v in cfg.items()}
+        if dkey is not None:  # one device copy of the sphere workload for all cells
+            for k in ("_src_d", "_q_d", "_trg_d"):
+                if k in c5:
+                    cfg[k] = c5[k]
+        precs = [F.PREC_MIXED, F.PREC_FP64]
+        if cfg["eps"] < 1e-6 and name != "config2":
+            precs = [F.PREC_FP64]
+        cell = {"name": name, "N": cfg["sources"].shape[0],
+                "M": 0 if cfg.get("targets") is None else cfg["targets"].shape[0],
+                "delta": cfg["delta"], "eps": cfg["eps"], "dim": cfg["dim"], "nd": cfg["nd"],
+                "iperiod": cfg["iperiod"], "ifpgh": cfg["ifpgh"], "ifpghtarg": cfg["ifpghtarg"],
+                "runs": []}
+        try:
+            for prec in precs:
+                steps = max(2, min(a.steps, 5))
+                r = run_cell(F, dev, stream, cfg, prec, steps, 2)
+                if dkey is not None:
+                    for k in ("_src_d", "_q_d", "_trg_d"):
+                        c5[k] = cfg[k]
+                key = (dkey, cfg["delta"]) if dkey is not None else name
+                if key not in exact_cache:
+                    exact_cache[key] = exact_for(F, dev, stream, cfg)
+                ex = exact_cache[key]
+                r2 = run_cell(F, dev, stream, cfg, prec, 1, 0, exact=ex)
+                r["rel_l2"] = r2["rel_l2"]
+                r.pop("_outputs", None)
+                del r2
+                cell["runs"].append(r)
+            if len(cell["runs"]) == 2:
+                cell["mixed_speedup"] = cell["runs"][1]["ms"] / cell["runs"][0]["ms"]
+        except Exception as ex:  # keep the other cells
+            cell["error"] = repr(ex)[:300]
+        torch.cuda.synchronize()
+        cells.append(cell)
+        print("sweep:", json.dumps(cell), file=sys.stderr, flush=True)
+    return cells
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -258,6 +460,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     stream = torch.cuda.current_stream()
     prec = F.PREC_MIXED if a.precision == "mixed" else F.PREC_FP64
+    if a.sweep_only:
+        cells = sweep(a, F, dev, stream, W)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "sweep": cells}), flush=True)
+        return
 
     # device-resident inputs and outputs (reference layouts, FP64)
     src_d = torch.from_numpy(cfg["sources"]).to(dev)
@@ -535,6 +742,11 @@ def main():
                  "note": "default worker count; sequential = the same call with one worker"}
         del keepb
 
+    cells = None
+    if a.sweep != "none" and world == 1:
+        del src_d, trg_d, q_d, pot_d, grad_d, pt_d, gt_d
+        torch.cuda.empty_cache()
+        cells = sweep(a, F, dev, stream, W)
     roof = roofline(a, stats, ms_phase)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -545,7 +757,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if a.precision == "mixed" else "f64", "data": "synthetic",
             "config": config, "clocks": clocks, "e2e": e2e, "roofline": roof,
-            "cpu_baseline": cpu, "accuracy": acc, "batch": batch, "plan": plan,
+            "cpu_baseline": cpu, "accuracy": acc, "batch": batch, "plan": plan, "sweep": cells,
             "gpu_launches": int(stats["n_kernel_launches"]) * a.steps,
             "phases_ms": {k: round(float(v), 4) for k, v in zip(
                 ["h2d", "tree", "sort_gather", "lists", "form", "translate", "eval", "direct",

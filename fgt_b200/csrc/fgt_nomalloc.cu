@@ -16,7 +16,11 @@
 // caller's outputs at the end.  Every call shares it: calls that overlap on
 // the GPU (on any streams) race.  In host code `g_scratch` only names the
 // symbol; its device address comes from cudaGetSymbolAddress, resolved once
-// per device by the first call made with that device current.
+// per device by the first call made with that device current.  CUDA loads a
+// module's device memory lazily, so that first call is also when the GPU
+// reserves the array: make it (a call with nt = 0 does it and computes
+// nothing) before the host hands the GPU's memory to its pool and before
+// any stream capture.
 #include <algorithm>
 #include <mutex>
 
@@ -192,6 +196,18 @@ int direct_nomalloc(int nd, int dim, double delta, double dmax, const double* sh
               "outputs exceed the static scratch of fgt_direct_nomalloc "
               "(nt*nd*(1 + dim*[ifpgh>=2] + nhess*[ifpgh>=3]) * 8 bytes must be <= "
               "FGT_NOMALLOC_SCRATCH_BYTES = 8 MiB)");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    (void)cudaGetLastError();
+    FGT_REQUIRE(false, FGT_ERR_NODEVICE, "no CUDA device");
+  }
+  int dev = 0;
+  FGT_CUDA(cudaGetDevice(&dev));
+  // Resolved before the empty-call return: a call with nt = 0 or ns = 0
+  // loads this module on the device (its static scratch is reserved then)
+  // and looks up the address, so a host can make that warm-up call before
+  // it hands the GPU's memory to its own pool or starts a stream capture.
+  double* acc = scratch_on(dev);
   if (nt == 0 || ns == 0) return FGT_OK;
   FGT_REQUIRE(sources && targ && pot, FGT_ERR_ARG, "sources, targ and pot are required");
   FGT_REQUIRE(ifcharge != 1 || charge, FGT_ERR_ARG, "charge is required when ifcharge=1");
@@ -200,14 +216,6 @@ int direct_nomalloc(int nd, int dim, double delta, double dmax, const double* sh
   FGT_REQUIRE(ifpgh < 2 || grad, FGT_ERR_ARG, "grad is required when ifpgh>=2");
   FGT_REQUIRE(ifpgh < 3 || hess, FGT_ERR_ARG, "hess is required when ifpgh=3");
   if (ifcharge != 1 && ifdipole != 1) return FGT_OK;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-    (void)cudaGetLastError();
-    FGT_REQUIRE(false, FGT_ERR_NODEVICE, "no CUDA device");
-  }
-  int dev = 0;
-  FGT_CUDA(cudaGetDevice(&dev));
-  double* acc = scratch_on(dev);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   FGT_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * (npot + ngrad + nhess), s));
   Shift sh = {{0, 0, 0}};

@@ -210,8 +210,12 @@ void pfgt_direct_(const int *nd, const int *dim, const double *delta,
  * Scratch is a static device array of FGT_NOMALLOC_SCRATCH_BYTES that every
  * GPU loading the library holds until exit: nt*nd*(1 + dim*[ifpgh>=2] +
  * nhess*[ifpgh>=3]) doubles must fit in it, else FGT_ERR_UNSUPPORTED.  The
- * first call on each device resolves the array's address with
- * cudaGetSymbolAddress; make that first call before any stream capture.
+ * first call on each device loads the library's module there (CUDA loads
+ * modules lazily, so that is when the GPU reserves the array) and resolves
+ * the array's address with cudaGetSymbolAddress.  Make that first call
+ * before the host gives the GPU's memory to its own pool and before any
+ * stream capture; a call with nt = 0 or ns = 0 does exactly this and
+ * computes nothing.
  * All calls share the array (it is cleared at the start of each call):
  * calls that overlap on the GPU, on any streams, race.
  */

@@ -549,8 +549,18 @@ static void pw_nodes_periodic(double bsize0, double delta, int npw, double *ws,
 /* direct kernels, pfgt_direct.f:47-615                                     */
 /* ------------------------------------------------------------------------ */
 
-/* One source/target pair, all nine gnd_direct{c,d,cd}{p,g,h} variants
- * (pfgt_direct.f:47-615).  dr = t - s.  Output increments. */
+/* One source/target pair of the gnd_direct{c,d,cd}{p,g,h} kernels
+ * (pfgt_direct.f:47-615).  dr = t - s.  Output increments.
+ *
+ * One departure: with charges AND dipoles and ifpgh = 3, the reference's
+ * gnd_directcdh (pfgt_direct.f:510-598) forms the dipole Hessian from
+ * dg = (-2/delta) dr (the charge kernel's factor) in the formula written for
+ * dg = (+2/delta) dr, so the signs of its rinc and rincg terms are flipped
+ * and its dipole Hessian is not the Hessian of its dipole potential (the
+ * finite-difference test in tests/test_oracle.py shows it).  Here the dipole
+ * part always uses the gnd_directdh formulas (pfgt_direct.f:309-384), the
+ * true Hessian, as the reference's own dipole-only kernel and its
+ * plane-wave far field do. */
 static void direct_pair(int nd, int dim, double delta, double dmax,
                         const double *dr, int ifcharge, const double *q,
                         int ifdipole, const double *rn, const double *ds,

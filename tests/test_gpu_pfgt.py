@@ -57,10 +57,64 @@ def _case_list():
         ("2d_small_root_direct", dict(nd=1, dim=2, delta=1.0, eps=1e-6, iperiod=0,
                                       sources=u(rng, 50, 2) * 0.01,
                                       charge=rng.uniform(-1, 1, (50, 1)), ifpgh=2)),
+    ] + _benchmark_regime_cases()
+
+
+def _benchmark_regime_cases():
+    """Reduced-size cases in the regimes of the benchmark configurations:
+    3D at eps = 1e-9 and 1e-12 (npw 40 and 54; the FP64 grids exceed shared
+    memory, so form and evaluation run on global-memory grids), the
+    clustered sources with separate targets of configuration 2, the 2D
+    periodic multi-density field of configuration 3, 3D periodic (free-space
+    and periodic plane-wave nodes), several densities in 3D, and the
+    sphere + background point set at delta = 1e-1 (cut-off level 0: one
+    root box holds every point)."""
+    rng = np.random.default_rng(17)
+    u = W.uniform
+    c5 = W.config(5, scale=0.0005, delta=1e-1, eps=1e-6)
+    c5 = {k: v for k, v in c5.items() if k != "name"}
+    c5e3 = W.config(5, scale=0.002, delta=1e-1, eps=1e-3)
+    c5e3 = {k: v for k, v in c5e3.items() if k != "name"}
+    return [
+        ("3d_eps1e-9", dict(nd=1, dim=3, delta=1e-3, eps=1e-9, iperiod=0,
+                            sources=W.gaussian_clusters(rng, 6000, 3, ncl=4),
+                            charge=rng.uniform(-1, 1, (6000, 1)), ifpgh=2,
+                            targets=u(rng, 500, 3), ifpghtarg=2)),
+        ("3d_eps1e-12", dict(nd=1, dim=3, delta=1e-3, eps=1e-12, iperiod=0,
+                             sources=W.gaussian_clusters(rng, 2500, 3, ncl=3),
+                             charge=rng.uniform(-1, 1, (2500, 1)), ifpgh=2,
+                             targets=u(rng, 300, 3), ifpghtarg=1)),
+        ("config2_clusters_eps1e-9", dict(nd=1, dim=3, delta=1e-5, eps=1e-9, iperiod=0,
+                                          sources=W.gaussian_clusters(rng, 10000, 3, ncl=8),
+                                          charge=rng.standard_normal((10000, 1)), ifpgh=2,
+                                          targets=u(rng, 10000, 3), ifpghtarg=2)),
+        ("config3_periodic_nd4", dict(nd=4, dim=2, delta=1e-3, eps=1e-6, iperiod=1, bs0=1.0,
+                                      cen0=[0.0, 0.0], sources=u(rng, 20000, 2),
+                                      charge=rng.uniform(-1, 1, (20000, 4)), ifpgh=2)),
+        ("3d_periodic_pw", dict(nd=1, dim=3, delta=4e-3, eps=1e-6, iperiod=1, bs0=1.0,
+                                cen0=[0.0, 0.0, 0.0], sources=u(rng, 20000, 3),
+                                charge=rng.uniform(-1, 1, (20000, 1)), ifpgh=2)),
+        ("3d_periodic_nodes", dict(nd=1, dim=3, delta=1e-2, eps=1e-6, iperiod=1, bs0=1.0,
+                                   cen0=[0.0, 0.0, 0.0], sources=u(rng, 20000, 3),
+                                   charge=rng.uniform(-1, 1, (20000, 1)), ifpgh=2)),
+        ("3d_nd3", dict(nd=3, dim=3, delta=3e-3, eps=1e-6, iperiod=0,
+                        sources=W.gaussian_clusters(rng, 4000, 3, ncl=4),
+                        charge=rng.uniform(-1, 1, (4000, 3)), ifpgh=2,
+                        targets=u(rng, 400, 3), ifpghtarg=1)),
+        ("config5_delta1e-1_root", c5),
+        ("config5_delta1e-1_eps1e-3", c5e3),
     ]
 
 
 CASES = _case_list()
+_ORACLE = {}
+
+
+def oracle_result(oracle, name, kw):
+    """The oracle's output of a named case, computed once per session."""
+    if name not in _ORACLE:
+        _ORACLE[name] = oracle.pfgt(**kw)
+    return _ORACLE[name]
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: c[0])
@@ -69,7 +123,11 @@ def test_pfgt_matches_oracle(fgt, oracle, case, prec):
     name, kw = case
     p = fgt.PREC_FP64 if prec == "fp64" else fgt.PREC_MIXED
     r = fgt.pfgt(precision=p, stats=True, **kw)
-    ro = oracle.pfgt(**kw)
+    ro = oracle_result(oracle, name, kw)
+    if name in ("3d_eps1e-9", "3d_eps1e-12", "config2_clusters_eps1e-9", "3d_periodic_pw",
+                "3d_periodic_nodes", "3d_nd3", "config3_periodic_nd4",
+                "config5_delta1e-1_root", "config5_delta1e-1_eps1e-3"):
+        assert r["stats"]["n_form_boxes"] > 0, (name, r["stats"])  # the plane-wave path ran
     tol = 0.3 * kw["eps"] if prec == "fp64" else max(0.3 * kw["eps"], 1e-6)
     for f in FIELDS:
         if f in ro:

@@ -207,3 +207,62 @@ def test_golden_fixtures(oracle, fname):
     for f in ("pot", "grad", "pottarg", "gradtarg"):
         if f in d.files and f in r:
             np.testing.assert_allclose(r[f], d[f], rtol=1e-12, atol=1e-14)
+
+
+def _cdh_reference_hessian(dim, delta, src, q, rn, ds, trg):
+    """The Hessian of gnd_directcdh as the reference writes it
+    (src/pfgt/pfgt_direct.f:510-598, one density, no cut-off): the dipole
+    terms use dg = (-2/delta)(t - s) in the gnd_directdh formula."""
+    nh = dim * (dim + 1) // 2
+    pairs = [(k, k) for k in range(dim)] + [(k, j) for k in range(dim) for j in range(k + 1, dim)]
+    if dim == 2:
+        pairs = [(0, 0), (0, 1), (1, 1)]
+    rfac = -2.0 / delta
+    out = np.zeros((trg.shape[0], nh))
+    for t in range(trg.shape[0]):
+        dr = trg[t] - src
+        e = np.exp(-np.sum(dr * dr, axis=1) / delta)
+        dg = rfac * dr
+        rinc = -np.sum(dg * rn, axis=1)
+        rincg = -rn * rfac + rinc[:, None] * dg
+        for m, (k, j) in enumerate(pairs):
+            ch = (rfac if k == j else 0.0) + dg[:, k] * dg[:, j]
+            if k == j:
+                dh = -rfac * (dg[:, k] * rn[:, k] + rinc) - rincg[:, k] * dg[:, k]
+            else:
+                dh = -rfac * dg[:, k] * rn[:, j] - rincg[:, k] * dg[:, j]
+            out[t, m] = np.sum(e * (ch * q[:, 0] + dh * ds[:, 0]))
+    return out
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_combined_charge_dipole_hessian_is_the_true_hessian(oracle, dim):
+    """Charges and dipoles with hessians: the oracle (and the GPU library)
+    return the Hessian of the potential, checked here against central
+    differences of the gradient.  The reference's gnd_directcdh formula
+    differs from it (flipped rinc/rincg terms); the restatement of that
+    formula above must fail the same check, which documents the departure."""
+    rng = np.random.default_rng(31 + dim)
+    ns, nt, delta = 40, 6, 0.05
+    src = rng.uniform(-0.2, 0.2, (ns, dim))
+    q = rng.uniform(-1, 1, (ns, 1))
+    ds = rng.uniform(-1, 1, (ns, 1))
+    rn = rng.standard_normal((ns, dim))
+    trg = rng.uniform(-0.15, 0.15, (nt, dim))
+    kw = dict(charge=q, dipstr=ds, rnormal=rn)
+    r = oracle.direct_exact(1, dim, delta, src, trg, ifpgh=3, **kw)
+    h = 1e-5
+    pairs = [(k, k) for k in range(dim)] + [(k, j) for k in range(dim) for j in range(k + 1, dim)]
+    if dim == 2:
+        pairs = [(0, 0), (0, 1), (1, 1)]
+    fd = np.zeros((nt, len(pairs)))
+    for m, (k, j) in enumerate(pairs):
+        tp, tm = trg.copy(), trg.copy()
+        tp[:, j] += h
+        tm[:, j] -= h
+        gp = oracle.direct_exact(1, dim, delta, src, tp, ifpgh=2, **kw)["grad"][:, k, 0]
+        gm = oracle.direct_exact(1, dim, delta, src, tm, ifpgh=2, **kw)["grad"][:, k, 0]
+        fd[:, m] = (gp - gm) / (2 * h)
+    assert relerr(fd, r["hess"][:, :, 0]) < 1e-6
+    ref_cdh = _cdh_reference_hessian(dim, delta, src, q, rn, ds, trg)
+    assert relerr(fd, ref_cdh) > 1e-2

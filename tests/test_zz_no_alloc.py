@@ -36,16 +36,16 @@ def test_nomalloc_rejects_outputs_beyond_scratch(fgt):
     assert b"static scratch" in L.fgt_last_error()
 
 
-def _reference(L, dim, delta, dmax, shift, src, q, rn, ds, trg, pgh):
+def _reference(L, nd, dim, delta, dmax, shift, src, q, rn, ds, trg, pgh):
     """The existing entry point: pfgt_direct_ on host arrays (gfortran ABI)."""
     nt, nh = trg.shape[0], dim * (dim + 1) // 2
-    pot = np.zeros((nt, 1))
-    grad = np.zeros((nt, dim, 1))
-    hess = np.zeros((nt, nh, 1))
+    pot = np.zeros((nt, nd))
+    grad = np.zeros((nt, dim, nd))
+    hess = np.zeros((nt, nh, nd))
     i = lambda v: C.byref(C.c_int(v))
     d = lambda v: C.byref(C.c_double(v))
     p = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
-    L.pfgt_direct_(i(1), i(dim), d(delta), d(dmax), i(1 if shift is not None else 0),
+    L.pfgt_direct_(i(nd), i(dim), d(delta), d(dmax), i(1 if shift is not None else 0),
                    p(shift if shift is not None else np.zeros(dim)), i(1), i(src.shape[0]), i(1),
                    i(nt), p(src), i(1 if q is not None else 0), p(q), i(1 if ds is not None else 0),
                    p(rn), p(ds), p(trg), i(pgh), p(pot), p(grad), p(hess))
@@ -61,35 +61,46 @@ def test_nomalloc_matches_pfgt_direct_on_two_calls(fgt):
     dev = torch.device("cuda", 0)
     stream = torch.cuda.current_stream()
     rng = np.random.default_rng(11)
-    # Two different calls in a row: the second has fewer targets, another
-    # dimension and field set, so stale accumulators of the first would show.
+    # A call with no targets computes nothing; it only loads the module and
+    # resolves the scratch address (the warm-up a pool-owning host makes).
+    rc = f(1, 3, 1e-3, 1.0, None, 10, None, 1, None, 0, None, None, 0, None, 1, None, None,
+           None, C.c_void_p(stream.cuda_stream))
+    assert rc == 0, L.fgt_last_error()
+    # Calls in a row with different shapes: each has another target count,
+    # dimension, density count or field set than the one before, so stale
+    # accumulators of an earlier call would show.
     calls = [
-        dict(dim=3, ns=7000, nt=2500, pgh=3, charge=True, dipole=True, shift=None,
+        dict(nd=1, dim=3, ns=7000, nt=2500, pgh=3, charge=True, dipole=True, shift=None,
              delta=2e-3, dmax=2e-3 * np.log(1e16)),
-        dict(dim=2, ns=3000, nt=400, pgh=2, charge=True, dipole=False,
+        dict(nd=1, dim=2, ns=3000, nt=400, pgh=2, charge=True, dipole=False,
              shift=np.array([1.0, 0.0]), delta=5e-2, dmax=1e30),
+        dict(nd=2, dim=1, ns=2000, nt=900, pgh=1, charge=False, dipole=True, shift=None,
+             delta=1e-3, dmax=1e-3 * np.log(1e12)),
+        dict(nd=3, dim=3, ns=4000, nt=700, pgh=3, charge=True, dipole=False, shift=None,
+             delta=1e-2, dmax=1e30),
     ]
     for c in calls:
-        dim, ns, nt, pgh = c["dim"], c["ns"], c["nt"], c["pgh"]
+        nd, dim, ns, nt, pgh = c["nd"], c["dim"], c["ns"], c["nt"], c["pgh"]
         nh = dim * (dim + 1) // 2
         src = rng.uniform(-0.5, 0.5, (ns, dim))
         trg = rng.uniform(-0.5, 0.5, (nt, dim))
         if c["shift"] is not None:
             trg[:, 0] += 1.0  # targets near the shifted image of the sources
-        q = rng.uniform(-1, 1, (ns, 1)) if c["charge"] else None
+        q = rng.uniform(-1, 1, (ns, nd)) if c["charge"] else None
         rn = rng.standard_normal((ns, dim)) if c["dipole"] else None
-        ds = rng.uniform(-1, 1, (ns, 1)) if c["dipole"] else None
-        ref = _reference(L, dim, c["delta"], c["dmax"], c["shift"], src, q, rn, ds, trg, pgh)
+        ds = rng.uniform(-1, 1, (ns, nd)) if c["dipole"] else None
+        ref = _reference(L, nd, dim, c["delta"], c["dmax"], c["shift"], src, q, rn, ds, trg,
+                         pgh)
 
         t = lambda a: None if a is None else torch.from_numpy(np.ascontiguousarray(a)).to(dev)
         dsrc, dtrg, dq, drn, dds = t(src), t(trg), t(q), t(rn), t(ds)
-        pot = torch.zeros((nt, 1), dtype=torch.float64, device=dev)
-        grad = torch.zeros((nt, dim, 1), dtype=torch.float64, device=dev)
-        hess = torch.zeros((nt, nh, 1), dtype=torch.float64, device=dev)
+        pot = torch.zeros((nt, nd), dtype=torch.float64, device=dev)
+        grad = torch.zeros((nt, dim, nd), dtype=torch.float64, device=dev)
+        hess = torch.zeros((nt, nh, nd), dtype=torch.float64, device=dev)
         ptr = lambda a: None if a is None else a.data_ptr()
         sh = c["shift"]
         torch.cuda.synchronize()
-        rc = f(1, dim, c["delta"], c["dmax"],
+        rc = f(nd, dim, c["delta"], c["dmax"],
                None if sh is None else sh.ctypes.data_as(C.c_void_p), ns, ptr(dsrc),
                1 if q is not None else 0, ptr(dq), 1 if ds is not None else 0, ptr(drn), ptr(dds),
                nt, ptr(dtrg), pgh, ptr(pot), ptr(grad) if pgh >= 2 else None,
@@ -101,4 +112,4 @@ def test_nomalloc_matches_pfgt_direct_on_two_calls(fgt):
             if k + 1 > pgh:
                 continue
             assert np.abs(ref[k]).max() > 0
-            assert relerr(ref[k], got[k]) < TOL, (name, dim, relerr(ref[k], got[k]))
+            assert relerr(ref[k], got[k]) < TOL, (name, nd, dim, relerr(ref[k], got[k]))
