@@ -17,8 +17,10 @@ struct FormIO {
   int n_form, ns, nd, ncomp;  // ncomp: charge (1) and/or dipole (dim)
   int has_q, has_dip;
   const int *form_box, *s_lo, *s_hi;
-  const int* order;  // form slots, most sources first
-  int* next;         // work counter (zero at launch)
+  const WorkItem* items;  // form items, most sources first
+  const int* n_items;     // item count (device)
+  int max_items;          // upper bound of the item count (grid sizing)
+  int* next;              // work counter (zero at launch)
 };
 
 template <typename T>
@@ -26,6 +28,7 @@ struct FormPtrs {
   const double* off;     // sorted SoA FP64 offsets
   const T *q, *ds, *rn;  // sorted SoA
   T* mp;                 // [n_form][nd][nexp] complex
+  T* partial;            // [partial slots][nd][nexp] complex: parts of split boxes
 };
 
 // ------------------------------------------------ block-tiled spreading (3D)
@@ -236,18 +239,24 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
   load_tw(twf, a.twf, 2 * G * NFp);
   load_tw(twh, a.twh, 2 * G * NHp);
   __syncthreads();
-  // boxes in decreasing source count, each CTA takes the next one
+  // items in decreasing source count, each CTA takes the next one; the
+  // parts of a split box write partial expansions, summed by k_form_reduce
   __shared__ int s_next;
+  const int n_items = *io.n_items;
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) s_next = atomicAdd(io.next, 1);
     __syncthreads();
-    if (s_next >= io.n_form) break;
-    const int fb = io.order[s_next];
+    if (s_next >= n_items) break;
+    const WorkItem it = io.items[s_next];
+    const int fb = it.slot;
     const int box = io.form_box[fb];
-    const int p0 = io.s_lo[box], p1 = io.s_hi[box];
+    int p0, p1;
+    part_range(io.s_lo[box], io.s_hi[box], it.part, it.nparts, p0, p1);
+    T* mp_base = it.pslot >= 0 ? p.partial + (size_t)it.pslot * io.nd * 2 * g.nexp
+                               : p.mp + (size_t)fb * io.nd * 2 * g.nexp;
     for (int id = 0; id < io.nd; id++) {
-      T* mp = p.mp + ((size_t)fb * io.nd + id) * 2 * g.nexp;
+      T* mp = mp_base + (size_t)id * 2 * g.nexp;
       int first = 1;
       for (int comp = 0; comp < io.ncomp; comp++) {
         // comp 0 = charge when present; the others are dipole directions
@@ -341,6 +350,32 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
         __syncthreads();
       }
     }
+  }
+}
+
+// mp of every split form box = sum of its parts' partial expansions, in part
+// order (deterministic).  One thread per (split box, density, mode).
+template <typename T>
+__global__ void k_form_reduce(const SplitRec* __restrict__ rec, const int* __restrict__ n_split,
+                              int nd, int nexp, const T* __restrict__ partial, T* __restrict__ mp) {
+  using V = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+  const long long per = (long long)nd * nexp;
+  const long long total = (long long)(*n_split) * per;
+  const V* pv = reinterpret_cast<const V*>(partial);
+  V* mv = reinterpret_cast<V*>(mp);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const SplitRec r = rec[i / per];
+    const long long j = i % per;
+    V acc;
+    acc.x = T(0);
+    acc.y = T(0);
+    for (int q = 0; q < r.nparts; q++) {
+      const V v = pv[(long long)(r.pslot + q) * per + j];
+      acc.x += v.x;
+      acc.y += v.y;
+    }
+    mv[(long long)r.slot * per + j] = acc;
   }
 }
 
@@ -440,7 +475,7 @@ template <typename T, int DIM, int W>
 int launch_form(PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>& gs, cudaStream_t s) {
   size_t fix = fixed_smem(a, W, 1);
   size_t need = fix + sizeof(T) * (size_t)a.g.bufsz;
-  int grid = std::max(1, std::min(io.n_form, kSMs));
+  int grid = std::max(1, std::min(io.max_items, kSMs));
   if constexpr (std::is_same<T, float>::value && DIM == 3 && TB + W - 1 <= TP - 1) {
     const int nbd = (a.g.G - W + 1 + TB - 1) / TB;
     const size_t tneed = tiled_offset<T>(a.g.G, a.g.K) + sizeof(T) * (size_t)a.g.bufsz;
@@ -475,8 +510,10 @@ int form_w(int w, PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>
     case 10: return launch_form<T, DIM, 10>(a, io, fp, gs, s);
     case 12: return launch_form<T, DIM, 12>(a, io, fp, gs, s);
     case 14: return launch_form<T, DIM, 14>(a, io, fp, gs, s);
-    default: return launch_form<T, DIM, 16>(a, io, fp, gs, s);
+    case 16: return launch_form<T, DIM, 16>(a, io, fp, gs, s);
+    default: FGT_REQUIRE(false, FGT_ERR_UNSUPPORTED, "no form kernel for this width");
   }
+  return 0;
 }
 void legendre(int nq, std::vector<double>& xq, std::vector<double>& wq) {
   const double pi = 4.0 * atan(1.0);
@@ -628,7 +665,8 @@ int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>
   io.s_hi = src.hi;
   // longest-processing-time order of the form boxes (by source count) and a
   // work counter: the boxes' costs vary by several times, so a fixed
-  // round-robin assignment leaves CTAs idle at the end
+  // round-robin assignment leaves CTAs idle at the end.  Boxes above the
+  // split threshold are cut into parts of about thr sources.
   DBuf<uint64_t> okey(std::max(L.n_form, 1), s), otmp(std::max(L.n_form, 1), s);
   DBuf<uint32_t> oval(std::max(L.n_form, 1), s), vtmp(std::max(L.n_form, 1), s);
   DBuf<int> next(1, s);
@@ -640,7 +678,13 @@ int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>
     FGT_LAUNCH_CHECK();
     radix_sort(okey, oval, otmp, vtmp, L.n_form, LPT_BITS, s);
   }
-  io.order = reinterpret_cast<const int*>(oval.get());
+  const int thr = form_split_threshold(src.n);
+  ItemList il;
+  build_items(il, L.n_form, nullptr, oval, L.form_box, src.lo, src.hi, nullptr, nullptr, src.n,
+              thr, true, s);
+  io.items = il.items;
+  io.n_items = il.n_items;
+  io.max_items = il.max_items;
   io.next = next;
   FormPtrs<T> fp;
   fp.off = src.off;
@@ -648,11 +692,16 @@ int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>
   fp.ds = src.ds;
   fp.rn = src.rn;
   fp.mp = D.mp;
+  DBuf<T> part((size_t)std::max(il.max_partial, 1) * P.nd * 2 * P.nexp, s);
+  fp.partial = part;
   DBuf<T> gs;
   int n;
   if (P.dim == 1) n = form_w<T, 1>(P.w, a, io, fp, gs, s);
   else if (P.dim == 2) n = form_w<T, 2>(P.w, a, io, fp, gs, s);
   else n = form_w<T, 3>(P.w, a, io, fp, gs, s);
+  k_form_reduce<T><<<kSMs * 4, 256, 0, s>>>(il.split, il.n_split, P.nd, P.nexp, part, D.mp);
+  FGT_LAUNCH_CHECK();
+  n += 6;
   if (work) {
     DBuf<unsigned long long> c(1, s);
     c.zero();

@@ -857,6 +857,137 @@ __global__ void k_lpt_keys(int n, const int* __restrict__ count, const int* __re
   }
 }
 
+// Work items of the form and grid-evaluation kernels.  A box whose point
+// count exceeds the split threshold is cut into `nparts` contiguous point
+// ranges of about equal size, each a separate item, so one large box (at a
+// cut-off level 0 the root box holds every point) keeps every SM busy
+// instead of one.  The items of a box are consecutive and follow the
+// longest-processing-time order of the boxes.  pslot: slot of the item's
+// partial expansion (form items of split boxes), -1 otherwise.
+struct WorkItem {
+  int slot, part, nparts, pslot;
+};
+// A split form box: its form slot, first partial slot and part count.
+struct SplitRec {
+  int slot, pslot, nparts;
+};
+
+// Part count of entry i of a sorted slot list (entries at or beyond *count
+// get 0): ceil(points / thr) when the box holds more than thr points, else 1.
+// nsplit[i] = part count of split boxes, 0 otherwise.
+__global__ void k_item_parts(int n, const int* __restrict__ count, const uint32_t* __restrict__ order,
+                             const int* __restrict__ box, const int* __restrict__ lo0,
+                             const int* __restrict__ hi0, const int* __restrict__ lo1,
+                             const int* __restrict__ hi1, int thr, int* __restrict__ nparts,
+                             int* __restrict__ nsplit) {
+  const int m = count ? *count : n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int np = 0;
+    if (i < m) {
+      const int b = box[order[i]];
+      const long long c =
+          (long long)(hi0[b] - lo0[b]) + (lo1 ? (long long)(hi1[b] - lo1[b]) : 0);
+      np = c > thr ? (int)((c + thr - 1) / thr) : 1;
+    }
+    nparts[i] = np;
+    nsplit[i] = np > 1 ? np : 0;
+  }
+}
+
+// Items of every entry (offsets from exclusive scans of nparts and nsplit);
+// split boxes are also listed in `split` (order of the list unspecified; each
+// record carries its own slots, so results do not depend on it).
+__global__ void k_item_fill(int n, const int* __restrict__ count, const uint32_t* __restrict__ order,
+                            const int* __restrict__ nparts, const int* __restrict__ ioff,
+                            const int* __restrict__ poff, WorkItem* __restrict__ items,
+                            SplitRec* __restrict__ split, int* __restrict__ nsplit_total) {
+  const int m = count ? *count : n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const int np = nparts[i], slot = (int)order[i], o = ioff[i];
+    for (int p = 0; p < np; p++) {
+      WorkItem w;
+      w.slot = slot;
+      w.part = p;
+      w.nparts = np;
+      w.pslot = np > 1 ? poff[i] + p : -1;
+      items[o + p] = w;
+    }
+    if (np > 1 && split) {
+      const int k = atomicAdd(nsplit_total, 1);
+      SplitRec r;
+      r.slot = slot;
+      r.pslot = poff[i];
+      r.nparts = np;
+      split[k] = r;
+    }
+  }
+}
+
+// Split thresholds (points per part) of the form and grid-evaluation
+// kernels for a call with n points in the set: about two parts per SM when
+// every point sits in one box, never below the size at which the per-part
+// grid transforms stop being small against the spreading or interpolation.
+inline int form_split_threshold(long long n) {
+  return (int)std::max<long long>(8192, (n + 2 * kSMs - 1) / (2 * kSMs));
+}
+inline int eval_split_threshold(long long n) {
+  return (int)std::max<long long>(8192, (n + 2 * kSMs - 1) / (2 * kSMs));
+}
+
+// Work items of a sorted slot list (host side, all sizes stay on the device).
+// n: list length bound; count: actual length on the device (or null = n);
+// npts_bound: upper bound of the points over all listed boxes; thr: split
+// threshold.  Items and split records live in the call's workspace.
+struct ItemList {
+  DBuf<WorkItem> items;
+  DBuf<SplitRec> split;
+  DBuf<int> n_items, n_split, n_partial;
+  int max_items = 0, max_partial = 0;
+};
+inline void build_items(ItemList& il, int n, const int* count, const uint32_t* order,
+                        const int* box, const int* lo0, const int* hi0, const int* lo1,
+                        const int* hi1, long long npts_bound, int thr, bool want_split,
+                        cudaStream_t s) {
+  // every split box holds more than thr points and has at most 2*points/thr
+  // parts; every other box has one
+  const long long extra = 2 * (npts_bound / std::max(thr, 1)) + 1;
+  il.max_items = (int)std::min<long long>((long long)n + extra, 1ll << 30);
+  il.max_partial = (int)std::min<long long>(extra, 1ll << 30);
+  DBuf<int> np(std::max(n, 1), s), ns(std::max(n, 1), s), ioff(std::max(n, 1), s),
+      poff(std::max(n, 1), s);
+  il.items.alloc(std::max(il.max_items, 1), s);
+  il.n_items.alloc(1, s);
+  il.n_partial.alloc(1, s);
+  il.n_split.alloc(1, s);
+  il.n_split.zero();
+  if (want_split) il.split.alloc(std::max(il.max_partial, 1), s);
+  if (n <= 0) {
+    il.n_items.zero();
+    il.n_partial.zero();
+    return;
+  }
+  k_item_parts<<<grid_for(n, 256), 256, 0, s>>>(n, count, order, box, lo0, hi0, lo1, hi1, thr, np,
+                                                 ns);
+  FGT_LAUNCH_CHECK();
+  exclusive_scan_i32(np, ioff, n, il.n_items, s);
+  exclusive_scan_i32(ns, poff, n, il.n_partial, s);
+  k_item_fill<<<grid_for(n, 256), 256, 0, s>>>(n, count, order, np, ioff, poff, il.items,
+                                                want_split ? il.split.get() : nullptr, il.n_split);
+  FGT_LAUNCH_CHECK();
+}
+
+// Point range [q0, q1) of part `part` of `nparts` of [lo, hi).
+__device__ __forceinline__ void part_range(int lo, int hi, int part, int nparts, int& q0, int& q1) {
+  if (nparts <= 1) {
+    q0 = lo;
+    q1 = hi;
+    return;
+  }
+  const int chunk = (hi - lo + nparts - 1) / nparts;
+  q0 = min(hi, lo + part * chunk);
+  q1 = min(hi, q0 + chunk);
+}
+
 template <typename T>
 __device__ __forceinline__ void load_tw(T* dst, const T* src, int n) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];

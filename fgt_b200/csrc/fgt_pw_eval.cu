@@ -20,6 +20,10 @@ struct EvalPtrs {
   int nbox;             // upper bound (grid sizing)
   const int* nbox_dev;  // actual count on the device, or null: nbox
   int* next;            // work counter of the grid kernel (zero at launch)
+  // grid kernel: work items (parts of boxes), count on the device, bound
+  const WorkItem* items;
+  const int* n_items;
+  int max_items;
   // two evaluation sets (sources, targets)
   const double* off[2];
   const int* lo[2];
@@ -158,16 +162,18 @@ __global__ void __launch_bounds__(eval_threads<T, DIM, W, GB, DERIV>())
   const uint32_t grid_saddr =
       (uint32_t)__cvta_generic_to_shared(smem_raw) + (uint32_t)eval_offset<T>(G, K);
   (void)grid_saddr;
-  const int nbox = p.nbox_dev ? *p.nbox_dev : p.nbox;
-  // boxes in decreasing point count, each CTA takes the next one
+  const int n_items = *p.n_items;
+  // items (boxes, or parts of large boxes) in decreasing point count, each
+  // CTA takes the next one; a part evaluates its share of both point sets
   __shared__ int s_next;
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) s_next = atomicAdd(p.next, 1);
     __syncthreads();
     const int bi = s_next;
-    if (bi >= nbox) break;
-    const int e = p.boxes[bi];
+    if (bi >= n_items) break;
+    const WorkItem it = p.items[bi];
+    const int e = it.slot;
     const int box = p.eval_box[e];
     for (int id = 0; id < p.nd; id++) {
       const T* L = p.loc + ((size_t)e * p.nd + id) * 2 * g.nexp;
@@ -180,8 +186,9 @@ __global__ void __launch_bounds__(eval_threads<T, DIM, W, GB, DERIV>())
           if (c >= (set ? p.ncomp[1] : p.ncomp[0]) || ne == 0) continue;
           const double* offs = set ? p.off[1] : p.off[0];
           double* outs = set ? p.out[1] : p.out[0];
-          const int q0 = set ? p.lo[1][box] : p.lo[0][box];
-          const int q1 = set ? p.hi[1][box] : p.hi[0][box];
+          int q0, q1;
+          part_range(set ? p.lo[1][box] : p.lo[0][box], set ? p.hi[1][box] : p.hi[0][box],
+                     it.part, it.nparts, q0, q1);
           for (int c0 = q0; c0 < q1; c0 += ORDER_CHUNK) {
             const int n = min(ORDER_CHUNK, q1 - c0);
             if (p.cell_bins > 0)
@@ -576,7 +583,7 @@ template <typename T, int DIM, int W, bool DERIV>
 int launch_eval_k(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t s) {
   size_t fix = eval_offset<T>(a.g.G, a.g.K);
   size_t need = fix + sizeof(T) * (size_t)a.g.bufsz;
-  int grid = std::max(1, std::min(ep.nbox, kSMs));
+  int grid = std::max(1, std::min(ep.max_items, kSMs));
   bool gb = need > (size_t)MAXSMEM;
   EvalPtrs<T> epk = ep;
   {  // cell order when the sub-grid's base cells fit the bins
@@ -632,8 +639,10 @@ int eval_w(int w, PWArgs<T>& a, const EvalPtrs<T>& ep, bool deriv, DBuf<T>& gs, 
     case 10: return launch_eval<T, DIM, 10>(a, ep, deriv, gs, s);
     case 12: return launch_eval<T, DIM, 12>(a, ep, deriv, gs, s);
     case 14: return launch_eval<T, DIM, 14>(a, ep, deriv, gs, s);
-    default: return launch_eval<T, DIM, 16>(a, ep, deriv, gs, s);
+    case 16: return launch_eval<T, DIM, 16>(a, ep, deriv, gs, s);
+    default: FGT_REQUIRE(false, FGT_ERR_UNSUPPORTED, "no evaluation kernel for this width");
   }
+  return 0;
 }
 template <typename T>
 int eval_dim(int dim, int w, PWArgs<T>& a, const EvalPtrs<T>& ep, bool deriv, DBuf<T>& gs,
@@ -660,7 +669,11 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   // requested or w+2 exceeds the widest kernel.
   // FP32: width w+1 (its aliasing error, ~1e-7 at eps = 1e-6, stays below
   // the FP32 rounding of the sums); FP64: w+2
-  const int wgrad = P.w + (sizeof(T) == 4 ? 1 : 2);
+  // The evaluation kernels exist for widths 6..10, 12, 14 and 16 (odd
+  // widths 7 and 9 for the FP32 derivative only): an odd width above 9
+  // (FP32 at eps < 1e-6) is rounded up to the next even one.
+  int wgrad = P.w + (sizeof(T) == 4 ? 1 : 2);
+  if (wgrad > 9 && (wgrad & 1)) wgrad++;
   const bool deriv = pgh_max == 2 && wgrad <= 16;
   const int mode = deriv ? 1 : 2;
   PWParams Pe = P;
@@ -710,6 +723,10 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
     ep.ncomp[i] = us[i] ? ncomp(es[i]->pgh) : 0;
   }
   ep.ncomp_max = std::max(ep.ncomp[0], ep.ncomp[1]);
+  ep.items = nullptr;
+  ep.n_items = nullptr;
+  ep.max_items = 0;
+  ItemList il;
   DBuf<T> gs;
   {
     // longest-processing-time order of the grid boxes (by point count)
@@ -727,7 +744,15 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
     ep.nbox = L.n_eval;
     ep.nbox_dev = counts.get();
     ep.next = next;
-    launches += 2 + eval_dim<T>(P.dim, Pe.w, a, ep, deriv, gs, s);
+    // boxes above the split threshold become several items
+    const long long npts = (u0 ? (long long)e0.n : 0) + (u1 ? (long long)e1.n : 0);
+    build_items(il, L.n_eval, counts.get(), reinterpret_cast<const uint32_t*>(lbig.get()),
+                L.eval_box, u0 ? e0.lo : e1.lo, u0 ? e0.hi : e1.hi, (u0 && u1) ? e1.lo : nullptr,
+                (u0 && u1) ? e1.hi : nullptr, npts, eval_split_threshold(npts), false, s);
+    ep.items = il.items;
+    ep.n_items = il.n_items;
+    ep.max_items = il.max_items;
+    launches += 6 + eval_dim<T>(P.dim, Pe.w, a, ep, deriv, gs, s);
   }
   {
     ep.boxes = lsmall;
