@@ -45,7 +45,7 @@ def parse():
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--profile-once", action="store_true",
                    help="one untimed step only (for ncu launch lists)")
-    p.add_argument("--sweep", default="none", choices=["none", "cells", "all"],
+    p.add_argument("--sweep", default="cells", choices=["none", "cells", "all"],
                    help="also time the benchmark's other configurations: 'cells' = the "
                         "delta/eps cells of the sphere workload at eps=1e-6 plus configs 1-3, "
                         "'all' = every delta x eps cell")
@@ -199,8 +199,8 @@ def cpu_reference(cfg, target_s=10.0, frac=None):
         s = src[idx]
         q = cfg["charge"][idx]
         t0 = time.perf_counter()
-        O.pfgt(cfg["nd"], 3, cfg["delta"], cfg["eps"], 0, s, charge=q, ifpgh=cfg["ifpgh"],
-               targets=s.copy(), ifpghtarg=cfg["ifpghtarg"], nufft="spread")
+        out = O.pfgt(cfg["nd"], 3, cfg["delta"], cfg["eps"], 0, s, charge=q, ifpgh=cfg["ifpgh"],
+                     targets=s.copy(), ifpghtarg=cfg["ifpghtarg"], nufft="spread")
         t = time.perf_counter() - t0
         if t >= 0.3 * target_s or frac >= 0.05:
             break
@@ -208,7 +208,32 @@ def cpu_reference(cfg, target_s=10.0, frac=None):
     npts = 2 * len(idx)
     desc = (f"{len(idx)} sources + {len(idx)} targets (same points) inside a cube of the "
             f"workload, {t:.2f} s per run, nufft=spread")
+    cpu_reference.last = (idx, out)
     return npts / t, desc, O.threads(), frac
+
+
+def window_parity(F, cfg, prec, idx, ref_out, nexact=200):
+    """The GPU path on the CPU baseline's window (same points, charges and
+    parameters) against the restatement's output there, and both against the
+    exact FP64 sum over the window's sources at `nexact` window points."""
+    from oracle import oracle as O
+    s = cfg["sources"][idx]
+    q = cfg["charge"][idx]
+    r = F.pfgt(cfg["nd"], 3, cfg["delta"], cfg["eps"], 0, s, charge=q, ifpgh=cfg["ifpgh"],
+               targets=s.copy(), ifpghtarg=cfg["ifpghtarg"], precision=prec)
+    out = {"points": int(len(idx)), "gpu_vs_restatement": {
+        "pot": O.relerr(ref_out["pot"], r["pot"]), "grad": O.relerr(ref_out["grad"], r["grad"]),
+        "pottarg": O.relerr(ref_out["pottarg"], r["pottarg"]),
+        "gradtarg": O.relerr(ref_out["gradtarg"], r["gradtarg"])}}
+    k = np.random.default_rng(3).choice(len(idx), min(nexact, len(idx)), replace=False)
+    ex = O.direct_exact(cfg["nd"], 3, cfg["delta"], s, s[k], charge=q, ifpgh=2)
+    out["vs_exact"] = {
+        "sample": f"{len(k)} window points, FP64 direct sum over the window's sources (CPU)",
+        "restatement": {"pot": O.relerr(ex["pot"], ref_out["pot"][k]),
+                        "grad": O.relerr(ex["grad"], ref_out["grad"][k])},
+        "gpu": {"pot": O.relerr(ex["pot"], r["pot"][k]),
+                "grad": O.relerr(ex["grad"], r["grad"][k])}}
+    return out
 
 
 def _ptr(t):
@@ -585,6 +610,23 @@ def main():
 
         acc = {"reference": "FP64 direct sum over all sources (no cut-off), GPU all-pairs kernel",
                "sample": f"{ns_s} sources + {ns_t} targets", "rel_l2": errs()}
+        if rank == 0 and world == 1 and not a.no_cpu:
+            # the GPU all-pairs reference itself checked by the CPU oracle's
+            # exact sum over all N sources at a few of the sampled points
+            from oracle import oracle as O
+            kx = 32
+            pts = src_d[i_s[:kx]].cpu().numpy()
+            t0 = time.perf_counter()
+            ce = O.direct_exact(1, 3, cfg["delta"], cfg["sources"], pts, charge=cfg["charge"],
+                                ifpgh=2)
+            acc["cpu_exact_crosscheck"] = {
+                "points": kx, "seconds": round(time.perf_counter() - t0, 2),
+                "gpu_allpairs_vs_cpu_exact": {
+                    "pot": O.relerr(ce["pot"], xs_p[:kx].cpu().numpy()),
+                    "grad": O.relerr(ce["grad"], xs_g[:kx].cpu().numpy())},
+                "fast_path_vs_cpu_exact": {
+                    "pot": O.relerr(ce["pot"], pot_d[i_s[:kx]].cpu().numpy()),
+                    "grad": O.relerr(ce["grad"], grad_d[i_s[:kx]].cpu().numpy())}}
         # the FP64 GPU path side by side: time and error on the same workload
         if world == 1 and a.precision == "mixed":
             mixed_out = [t.clone() for t in (pot_d, grad_d, pt_d, gt_d)]
@@ -748,10 +790,16 @@ def main():
         torch.cuda.empty_cache()
         cells = sweep(a, F, dev, stream, W)
     roof = roofline(a, stats, ms_phase)
+    if roof.get("traffic") is not None:
+        roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                                  "of the kernel on the 0.3-scale workload, scaled to this size "
+                                  "by points and boxes (profiles/ncu_traffic.json)")
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         v, desc, cores, _ = cpu_reference(cfg, target_s=12.0)
         cpu = {"value": v, "unit": "pts/s", "cores": cores, "kind": "port", "sample": desc}
+        widx, wout = cpu_reference.last
+        cpu["window_parity"] = window_parity(F, cfg, prec, widx, wout)
     line = {"metric": METRIC, "value": value, "unit": "pts/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

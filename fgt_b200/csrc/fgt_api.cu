@@ -253,18 +253,41 @@ struct Setup {
   int launches = 0;
 };
 
-// Records of the packed list-1 sources are 64 bytes; above this count (4 GiB)
-// the near field walks the list instead.  FGT_NEAR_PACK_MAX (a record count,
-// 0 = never pack) lowers the cap, e.g. to test the list-walking kernel.
-constexpr long long kMaxNearRecords = 1ll << 26;
+// Records of the packed list-1 sources are 64 bytes; above this count (16 GiB,
+// and at most an eighth of the device's memory) the near field walks the
+// list instead.  The cap depends only on the device, so repeated calls take
+// the same path and reuse the same workspace.  FGT_NEAR_PACK_MAX (a record
+// count, 0 = never pack) lowers it, e.g. to test the list-walking kernel.
+constexpr long long kMaxNearRecords = 1ll << 28;
 long long near_pack_max() {
+  static std::mutex mu;
+  static long long caps[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    (void)cudaGetLastError();
+    dev = 0;
+  }
+  long long cap;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (caps[dev] == 0) {
+      size_t free_b = 0, total_b = 0;
+      long long c = kMaxNearRecords;
+      if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
+        c = std::min(c, (long long)(total_b / 8 / 64));
+      else
+        (void)cudaGetLastError();
+      caps[dev] = std::max(c, 1ll);
+    }
+    cap = caps[dev];
+  }
   const char* e = getenv("FGT_NEAR_PACK_MAX");
   if (e && *e) {
     char* end = nullptr;
     const long long v = strtoll(e, &end, 10);
-    if (end != e && v >= 0) return std::min(v, kMaxNearRecords);
+    if (end != e && v >= 0) return std::min(v, cap);
   }
-  return kMaxNearRecords;
+  return cap;
 }
 
 DirectGeom direct_geom(const Setup& u) {

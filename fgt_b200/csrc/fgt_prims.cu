@@ -140,7 +140,8 @@ constexpr int RS_ITEMS = 16;
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
 constexpr int RS_WARPS = RS_THREADS / 32;
 
-__global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const uint64_t* __restrict__ keys, int n,
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const K* __restrict__ keys, int n,
                                                            int shift, int* __restrict__ hist,
                                                            int nblocks) {
   __shared__ int h[256];
@@ -149,15 +150,16 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const uint64_t* __res
   int base = blockIdx.x * RS_TILE;
   for (int r = 0; r < RS_ITEMS; r++) {
     int i = base + r * RS_THREADS + threadIdx.x;
-    if (i < n) atomicAdd(&h[(int)((keys[i] >> shift) & 255ull)], 1);
+    if (i < n) atomicAdd(&h[(int)((keys[i] >> shift) & K(255))], 1);
   }
   __syncthreads();
   hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
+template <typename K>
 __global__ void __launch_bounds__(RS_THREADS)
-    k_radix_scatter(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
-                    uint64_t* __restrict__ kout, uint32_t* __restrict__ vout, int n, int shift,
+    k_radix_scatter(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
+                    K* __restrict__ kout, uint32_t* __restrict__ vout, int n, int shift,
                     const int* __restrict__ offs, int nblocks) {
   __shared__ int base[256];
   __shared__ int wc[RS_WARPS][256];
@@ -169,9 +171,9 @@ __global__ void __launch_bounds__(RS_THREADS)
   for (int r = 0; r < RS_ITEMS; r++) {
     int i = tbase + r * RS_THREADS + tid;
     bool valid = i < n;
-    uint64_t k = valid ? kin[i] : 0ull;
+    K k = valid ? kin[i] : K(0);
     uint32_t v = (valid && vin) ? vin[i] : 0u;
-    int d = valid ? (int)((k >> shift) & 255ull) : 256;
+    int d = valid ? (int)((k >> shift) & K(255)) : 256;
     unsigned peers = __match_any_sync(0xffffffffu, d);
     int rank = __popc(peers & lt);
     bool leader = (__ffs(peers) - 1) == lane;
@@ -237,28 +239,40 @@ void exclusive_scan_i32(const int* in, int* out, int n, int* total, cudaStream_t
   FGT_LAUNCH_CHECK();
 }
 
-void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* ktmp, uint32_t* vtmp, int n, int bits,
-                cudaStream_t s) {
+namespace {
+template <typename K>
+void radix_sort_t(K* keys, uint32_t* vals, K* ktmp, uint32_t* vtmp, int n, int bits,
+                  cudaStream_t s) {
   if (n <= 1 || bits <= 0) return;
   int nb = ceil_div(n, RS_TILE);
   DBuf<int> hist((size_t)256 * nb, s);
-  uint64_t *ka = keys, *kb = ktmp;
+  K *ka = keys, *kb = ktmp;
   uint32_t *va = vals, *vb = vtmp;
   int passes = 0;
   for (int shift = 0; shift < bits; shift += 8) {
-    k_radix_hist<<<nb, RS_THREADS, 0, s>>>(ka, n, shift, hist, nb);
+    k_radix_hist<K><<<nb, RS_THREADS, 0, s>>>(ka, n, shift, hist, nb);
     FGT_LAUNCH_CHECK();
     exclusive_scan_i32(hist, hist, 256 * nb, nullptr, s);
-    k_radix_scatter<<<nb, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, shift, hist, nb);
+    k_radix_scatter<K><<<nb, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, shift, hist, nb);
     FGT_LAUNCH_CHECK();
     std::swap(ka, kb);
     std::swap(va, vb);
     passes++;
   }
   if (passes & 1) {
-    FGT_CUDA(cudaMemcpyAsync(keys, ka, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, s));
+    FGT_CUDA(cudaMemcpyAsync(keys, ka, sizeof(K) * n, cudaMemcpyDeviceToDevice, s));
     if (vals) FGT_CUDA(cudaMemcpyAsync(vals, va, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
   }
+}
+}  // namespace
+
+void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* ktmp, uint32_t* vtmp, int n, int bits,
+                cudaStream_t s) {
+  radix_sort_t<uint64_t>(keys, vals, ktmp, vtmp, n, bits, s);
+}
+void radix_sort_u32(uint32_t* keys, uint32_t* vals, uint32_t* ktmp, uint32_t* vtmp, int n,
+                    int bits, cudaStream_t s) {
+  radix_sort_t<uint32_t>(keys, vals, ktmp, vtmp, n, bits, s);
 }
 
 void lower_bound_u64(const uint64_t* sorted, int n, const uint64_t* q, int m, int* out,

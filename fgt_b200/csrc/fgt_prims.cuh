@@ -87,6 +87,10 @@ void exclusive_scan_i32(const int* in, int* out, int n, int* total, cudaStream_t
 void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* ktmp, uint32_t* vtmp, int n,
                 int bits, cudaStream_t s);
 
+// The same on 32-bit keys (bits <= 32).
+void radix_sort_u32(uint32_t* keys, uint32_t* vals, uint32_t* ktmp, uint32_t* vtmp, int n,
+                    int bits, cudaStream_t s);
+
 // out[i] = lower_bound(sorted, n, q[i]) for m queries.
 void lower_bound_u64(const uint64_t* sorted, int n, const uint64_t* q, int m, int* out,
                      cudaStream_t s);

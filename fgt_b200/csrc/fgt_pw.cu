@@ -45,11 +45,6 @@ constexpr int FCH = 8192;       // points sorted per round
 constexpr int PB = 8;           // points per warp batch
 constexpr int TP = 12;          // padded kernel row (TILE <= TP - 1)
 
-// twiddle tables, rounded up to 16 bytes (the tiled scratch follows)
-template <typename T>
-__host__ __device__ constexpr size_t tw_bytes16(int G, int K) {
-  return ((size_t)sizeof(T) * tw_elems(G, K) + 15) & ~(size_t)15;
-}
 // byte offset of the grid buffer in the tiled form kernel; every part is a
 // multiple of 16 bytes, so the kernel-row buffer is float4 aligned
 template <typename T>
@@ -353,6 +348,124 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
   }
 }
 
+// Form of small 2D boxes, one warp per box (see small2_layout): the boxes
+// order[first..n_form) of the longest-processing-time order, which all hold
+// at most SMALL2_MAX sources.  Same sums as k_form for DIM = 2.
+template <typename T, int W>
+__global__ void __launch_bounds__(256) k_form_small2(PWArgs<T> a, FormIO io, FormPtrs<T> p,
+                                                     const uint32_t* __restrict__ order,
+                                                     const int* __restrict__ first,
+                                                     int* __restrict__ next) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Geo& g = a.g;
+  const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
+  T* twf = reinterpret_cast<T*>(smem_raw);
+  T* twh = twf + 2 * G * pad4(NF);
+  load_tw(twf, a.twf, 2 * G * pad4(NF));
+  load_tw(twh, a.twh, 2 * G * pad4(NH));
+  const Small2Layout lay = small2_layout(G, K);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* A = reinterpret_cast<T*>(smem_raw + tw_bytes16<T>(G, K)) + (size_t)warp * lay.per_warp;
+  T* Cb = A + lay.r1;
+  __syncthreads();
+  const int f0 = *first;
+  for (;;) {
+    int bi = 0;
+    if (lane == 0) bi = atomicAdd(next, 1);
+    bi = __shfl_sync(0xffffffffu, bi, 0) + f0;
+    if (bi >= io.n_form) break;
+    const int fb = (int)order[bi];
+    const int box = io.form_box[fb];
+    const int p0 = io.s_lo[box], p1 = io.s_hi[box];
+    for (int id = 0; id < io.nd; id++) {
+      T* mp = p.mp + ((size_t)fb * io.nd + id) * 2 * g.nexp;
+      for (int comp = 0; comp < io.ncomp; comp++) {
+        const bool is_q = io.has_q && comp == 0;
+        const int dd = is_q ? -1 : comp - io.has_q;
+        for (int i = lane; i < G * lay.SA; i += 32) A[i] = T(0);
+        __syncwarp();
+        // points in batches of 32: lane j prepares point j (stencil base,
+        // kernel offsets, strength), then the warp adds them one by one
+        for (int c0 = p0; c0 < p1; c0 += 32) {
+          const int nb = min(32, p1 - c0);
+          int bx = 0, by = 0;
+          T fx = T(0), fy = T(0), st = T(0);
+          if (lane < nb) {
+            const int pt = c0 + lane;
+            const double x = p.off[pt] * a.scale_d, y = p.off[(size_t)io.ns + pt] * a.scale_d;
+            bx = kernel_start<T>(a, x, fx) - g.l0;
+            by = kernel_start<T>(a, y, fy) - g.l0;
+            // cells beyond the sub-grid carry zero weight (points lie
+            // inside it), so the clamp only keeps the stencil in bounds
+            bx = bx < 0 ? 0 : (bx > G - W ? G - W : bx);
+            by = by < 0 ? 0 : (by > G - W ? G - W : by);
+            st = is_q ? p.q[(size_t)id * io.ns + pt]
+                      : p.ds[(size_t)id * io.ns + pt] * p.rn[(size_t)dd * io.ns + pt];
+          }
+          for (int j = 0; j < nb; j++) {
+            const int jbx = __shfl_sync(0xffffffffu, bx, j), jby = __shfl_sync(0xffffffffu, by, j);
+            const T jfx = __shfl_sync(0xffffffffu, fx, j), jfy = __shfl_sync(0xffffffffu, fy, j);
+            const T jst = __shfl_sync(0xffffffffu, st, j);
+            T v = T(0);
+            if (lane < 2 * W) {
+              const int k = lane < W ? lane : lane - W;
+              v = es_kernel<T>(((lane < W ? jfx : jfy) + (T)k) * a.inv_hw, a.beta);
+            }
+#pragma unroll
+            for (int cc = 0; cc < (W * W + 31) / 32; cc++) {
+              const int c = cc * 32 + lane;
+              const int cx = c < W * W ? c / W : 0, cy = c < W * W ? c % W : 0;
+              const T px = __shfl_sync(0xffffffffu, v, cx);
+              const T py = __shfl_sync(0xffffffffu, v, W + cy);
+              if (c < W * W) A[(jbx + cx) * lay.SA + jby + cy] += jst * px * py;
+            }
+            __syncwarp();
+          }
+        }
+        warp_pass_r2c<T>(A, lay.SA, Cb, lay.SC, G, NH, twh);
+        __syncwarp();
+        const bool first_c = comp == 0;
+        warp_pass_c2c<T>(Cb, lay.SC, G, NF, NH, twf, [&](int kxi, int ky, T re, T im) {
+          const int ki[3] = {kxi, ky + K, 0};
+          const T f = a.facf[kxi] * a.facf[ky + K];
+          T vr = re * f, vi = im * f;
+          if (!is_q) {  // * (-i) ts(k_d) / sqrt(delta0)
+            const T cf = a.ts[sel3(ki, dd)] * a.inv_sqd0;
+            const T tr = vi * cf, ti = -vr * cf;
+            vr = tr;
+            vi = ti;
+          }
+          const int m = kxi * NH + ky;
+          if (first_c) {
+            mp[2 * m] = vr;
+            mp[2 * m + 1] = vi;
+          } else {
+            mp[2 * m] += vr;
+            mp[2 * m + 1] += vi;
+          }
+        });
+        __syncwarp();
+      }
+    }
+  }
+}
+
+// First entry of a list sorted by k_lpt_keys (ascending keys = descending
+// point counts) whose box holds at most `limit` points.
+__global__ void k_first_at_most(const uint64_t* __restrict__ keys, int n, int limit,
+                                int* __restrict__ out) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    constexpr uint64_t MAXC = (1ull << (LPT_BITS - 1)) - 1;
+    const uint64_t v = MAXC - (uint64_t)limit;  // count <= limit  <=>  key >= v
+    int lo = 0, hi = n;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (keys[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    *out = lo;
+  }
+}
+
 // mp of every split form box = sum of its parts' partial expansions, in part
 // order (deterministic).  One thread per (split box, density, mode).
 template <typename T>
@@ -515,6 +628,42 @@ int form_w(int w, PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>
   }
   return 0;
 }
+// Shared memory of k_form_small2 and its warps per CTA (0: does not fit).
+template <typename T>
+int small2_warps(const Geo& g, size_t& smem) {
+  const Small2Layout lay = small2_layout(g.G, g.K);
+  const size_t fix = tw_bytes16<T>(g.G, g.K);
+  const size_t per = sizeof(T) * (size_t)lay.per_warp;
+  if (fix + per > (size_t)MAXSMEM) return 0;
+  const int nw = (int)std::min<size_t>(8, ((size_t)MAXSMEM - fix) / per);
+  smem = fix + per * nw;
+  return nw;
+}
+
+template <typename T, int W>
+void launch_form_small2(PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp,
+                        const uint32_t* order, const int* first, int* next, cudaStream_t s) {
+  size_t smem = 0;
+  const int nw = small2_warps<T>(a.g, smem);
+  auto k = k_form_small2<T, W>;
+  set_smem(k, smem);
+  k<<<kSMs * std::max(1, 8 / nw), 32 * nw, smem, s>>>(a, io, fp, order, first, next);
+  FGT_LAUNCH_CHECK();
+}
+template <typename T>
+void form_small2_w(int w, PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp,
+                   const uint32_t* order, const int* first, int* next, cudaStream_t s) {
+  switch (w) {
+    case 6: return launch_form_small2<T, 6>(a, io, fp, order, first, next, s);
+    case 8: return launch_form_small2<T, 8>(a, io, fp, order, first, next, s);
+    case 10: return launch_form_small2<T, 10>(a, io, fp, order, first, next, s);
+    case 12: return launch_form_small2<T, 12>(a, io, fp, order, first, next, s);
+    case 14: return launch_form_small2<T, 14>(a, io, fp, order, first, next, s);
+    case 16: return launch_form_small2<T, 16>(a, io, fp, order, first, next, s);
+    default: FGT_REQUIRE(false, FGT_ERR_UNSUPPORTED, "no form kernel for this width");
+  }
+}
+
 void legendre(int nq, std::vector<double>& xq, std::vector<double>& wq) {
   const double pi = 4.0 * atan(1.0);
   xq.resize(nq);
@@ -679,9 +828,19 @@ int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>
     radix_sort(okey, oval, otmp, vtmp, L.n_form, LPT_BITS, s);
   }
   const int thr = form_split_threshold(src.n);
+  // 2D: boxes with at most SMALL2_MAX sources (a suffix of the order) go to
+  // the warp-per-box kernel, the rest to the CTA kernel
+  size_t sm2 = 0;
+  const bool small2 = P.dim == 2 && !a.g.wrap && small2_warps<T>(a.g, sm2) > 0;
+  DBuf<int> first(1, s), next2(1, s);
+  if (small2) {
+    next2.zero();
+    k_first_at_most<<<1, 32, 0, s>>>(okey, L.n_form, SMALL2_MAX, first);
+    FGT_LAUNCH_CHECK();
+  }
   ItemList il;
-  build_items(il, L.n_form, nullptr, oval, L.form_box, src.lo, src.hi, nullptr, nullptr, src.n,
-              thr, true, s);
+  build_items(il, L.n_form, small2 ? first.get() : nullptr, oval, L.form_box, src.lo, src.hi,
+              nullptr, nullptr, src.n, thr, true, s);
   io.items = il.items;
   io.n_items = il.n_items;
   io.max_items = il.max_items;
@@ -699,6 +858,10 @@ int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>
   if (P.dim == 1) n = form_w<T, 1>(P.w, a, io, fp, gs, s);
   else if (P.dim == 2) n = form_w<T, 2>(P.w, a, io, fp, gs, s);
   else n = form_w<T, 3>(P.w, a, io, fp, gs, s);
+  if (small2) {
+    form_small2_w<T>(P.w, a, io, fp, oval, first, next2, s);
+    n += 2;
+  }
   k_form_reduce<T><<<kSMs * 4, 256, 0, s>>>(il.split, il.n_split, P.nd, P.nexp, part, D.mp);
   FGT_LAUNCH_CHECK();
   n += 6;

@@ -68,6 +68,12 @@ __host__ __device__ constexpr size_t tw_elems(int G, int K) {
                           : (size_t)pad4(G) * (3 * K + 2));
 }
 
+// twiddle tables, rounded up to 16 bytes (scratch or grids follow)
+template <typename T>
+__host__ __device__ constexpr size_t tw_bytes16(int G, int K) {
+  return ((size_t)sizeof(T) * tw_elems(G, K) + 15) & ~(size_t)15;
+}
+
 // byte offset of the grid buffer in shared memory: twiddles, then the
 // ordering scratch (ORDER_CHUNK ints + 32 counters + ORDER_CHUNK u16)
 template <typename T>
@@ -986,6 +992,111 @@ __device__ __forceinline__ void part_range(int lo, int hi, int part, int nparts,
   const int chunk = (hi - lo + nparts - 1) / nparts;
   q0 = min(hi, lo + part * chunk);
   q1 = min(hi, q0 + chunk);
+}
+
+// ------------------------------------------------ small 2D boxes, one warp each
+// A 2D box of the cut-off level with a few hundred points needs only
+// ~1e5 FMAs of spreading and passes: one CTA per box spends most of its time
+// in block barriers and shared-memory atomics.  These kernels give each box
+// to one warp: spreading walks the box's points in order with the lanes
+// owning the stencil's cells (plain read-modify-writes, no atomics), and the
+// line transforms are warp-wide register-blocked sums.  Per warp: the real
+// grid A (G rows of SA values, SA odd so lane-per-row accesses hit distinct
+// banks) and half-complex grids of SC values per row.  Region R1 holds the
+// real grid (form: spreading target; evaluation: the grid interpolated) or,
+// in the evaluation, first the modes (2K+1 rows); region R2 holds the G rows
+// of the half-complex intermediate of the two line passes.
+constexpr int SMALL2_MAX = 2048;  // points per box handled by a warp
+struct Small2Layout {
+  int SA, SC, r1, per_warp;  // r1, per_warp in elements
+};
+__host__ __device__ inline Small2Layout small2_layout(int G, int K) {
+  Small2Layout l;
+  l.SA = G | 1;
+  l.SC = (2 * (K + 1)) | 1;
+  const int a = G * l.SA, b = (2 * K + 1) * l.SC;
+  l.r1 = ((a > b ? a : b) + 3) & ~3;
+  l.per_warp = (l.r1 + G * l.SC + 3) & ~3;
+  return l;
+}
+
+// Pass along the last dimension, real -> half complex (form):
+// C[r][2k..2k+1] = sum_y A[r][y] tw[y][k], k < NH, lane r < G.
+template <typename T>
+__device__ __forceinline__ void warp_pass_r2c(const T* A, int SA, T* C, int SC, int G, int NH,
+                                              const T* tw) {
+  const int np = pad4(NH), lane = threadIdx.x & 31;
+  for (int r = lane; r < G; r += 32) {
+    const T* a = A + r * SA;
+    for (int k0 = 0; k0 < NH; k0 += 4) {
+      T re[4] = {T(0), T(0), T(0), T(0)}, im[4] = {T(0), T(0), T(0), T(0)};
+      const T* t = tw + k0;
+      for (int y = 0; y < G; y++, t += 2 * np) {
+        const T g = a[y];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          re[j] += g * t[j];
+          im[j] += g * t[np + j];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (k0 + j < NH) {
+          C[r * SC + 2 * (k0 + j)] = re[j];
+          C[r * SC + 2 * (k0 + j) + 1] = im[j];
+        }
+    }
+  }
+}
+
+// Pass along the last dimension, half complex -> real (evaluation):
+// A[r][y] = sum_k Re(C[r][k] tw[k][y]), y < G, lane r < G.
+template <typename T>
+__device__ __forceinline__ void warp_pass_c2r(const T* C, int SC, T* A, int SA, int G, int NH,
+                                              const T* tw) {
+  const int np = pad4(G), lane = threadIdx.x & 31;
+  for (int r = lane; r < G; r += 32) {
+    const T* c = C + r * SC;
+    for (int y0 = 0; y0 < G; y0 += 4) {
+      T acc[4] = {T(0), T(0), T(0), T(0)};
+      const T* t = tw + y0;
+      for (int k = 0; k < NH; k++, t += 2 * np) {
+        const T cr = c[2 * k], ci = c[2 * k + 1];
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[j] += cr * t[j] - ci * t[np + j];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (y0 + j < G) A[r * SA + y0 + j] = acc[j];
+    }
+  }
+}
+
+// Complex pass along the first dimension over the NH columns of C:
+// out(o, k) = sum_i C[i][k] tw[i][o], o < nout, i < nin; the lanes take
+// (column, group of 4 outputs) pairs and hand every finished group to
+// emit(o, k, re, im).
+template <typename T, class F>
+__device__ __forceinline__ void warp_pass_c2c(const T* C, int SC, int nin, int nout, int NH,
+                                              const T* tw, F&& emit) {
+  const int np = pad4(nout), ng = (nout + 3) / 4, lane = threadIdx.x & 31;
+  for (int pr = lane; pr < NH * ng; pr += 32) {
+    const int k = pr / ng, o0 = (pr - k * ng) * 4;
+    T re[4] = {T(0), T(0), T(0), T(0)}, im[4] = {T(0), T(0), T(0), T(0)};
+    const T* c = C + 2 * k;
+    const T* t = tw + o0;
+    for (int i = 0; i < nin; i++, c += SC, t += 2 * np) {
+      const T xr = c[0], xi = c[1];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        re[j] += xr * t[j] - xi * t[np + j];
+        im[j] += xr * t[np + j] + xi * t[j];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (o0 + j < nout) emit(o0 + j, k, re[j], im[j]);
+  }
 }
 
 template <typename T>

@@ -554,6 +554,106 @@ __global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal32(PWArgs<float> a,
   }
 }
 
+// Evaluation of small 2D boxes, one warp per box (see small2_layout): the
+// grid boxes boxes[first..*nbox_dev) of the longest-processing-time order,
+// which hold at most SMALL2_MAX points.  Potential only, or potential and
+// gradient through the kernel derivative (DERIV); same sums as k_eval_comp.
+template <typename T, int W, bool DERIV>
+__global__ void __launch_bounds__(256) k_eval_small2(PWArgs<T> a, EvalPtrs<T> p,
+                                                     const int* __restrict__ first,
+                                                     int* __restrict__ next) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Geo& g = a.g;
+  const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G, Gp = pad4(G);
+  T* tif = reinterpret_cast<T*>(smem_raw);
+  T* tih = tif + 2 * NF * Gp;
+  load_tw(tif, a.tif, 2 * NF * Gp);
+  load_tw(tih, a.tih, 2 * NH * Gp);
+  const Small2Layout lay = small2_layout(G, K);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* R1 = reinterpret_cast<T*>(smem_raw + tw_bytes16<T>(G, K)) + (size_t)warp * lay.per_warp;
+  T* R2 = R1 + lay.r1;
+  Geo gw = g;  // the warp's real grid: rows of SA values, y contiguous
+  gw.str[0] = lay.SA;
+  gw.str[1] = 1;
+  __syncthreads();
+  const int f0 = *first, nbox = *p.nbox_dev;
+  for (;;) {
+    int bi = 0;
+    if (lane == 0) bi = atomicAdd(next, 1);
+    bi = __shfl_sync(0xffffffffu, bi, 0) + f0;
+    if (bi >= nbox) break;
+    const int e = p.boxes[bi];
+    const int box = p.eval_box[e];
+    for (int id = 0; id < p.nd; id++) {
+      const T* L = p.loc + ((size_t)e * p.nd + id) * 2 * g.nexp;
+      for (int m = lane; m < g.nexp; m += 32) {
+        const int kxi = m / NH, ky = m - kxi * NH;
+        const T f = a.faci[kxi] * a.faci[ky + K];
+        R1[kxi * lay.SC + 2 * ky] = L[2 * m] * f;
+        R1[kxi * lay.SC + 2 * ky + 1] = L[2 * m + 1] * f;
+      }
+      __syncwarp();
+      warp_pass_c2c<T>(R1, lay.SC, NF, G, NH, tif, [&](int x, int ky, T re, T im) {
+        R2[x * lay.SC + 2 * ky] = re;
+        R2[x * lay.SC + 2 * ky + 1] = im;
+      });
+      __syncwarp();
+      warp_pass_c2r<T>(R2, lay.SC, R1, lay.SA, G, NH, tih);
+      __syncwarp();
+      const T* B = R1;
+      for (int set = 0; set < 2; set++) {
+        const int ne = set ? p.n[1] : p.n[0];
+        const int nc = set ? p.ncomp[1] : p.ncomp[0];
+        if (nc == 0 || ne == 0) continue;
+        const double* offs = set ? p.off[1] : p.off[0];
+        double* outs = set ? p.out[1] : p.out[0];
+        const int q0 = set ? p.lo[1][box] : p.lo[0][box];
+        const int q1 = set ? p.hi[1][box] : p.hi[0][box];
+        for (int q = q0 + lane; q < q1; q += 32) {
+          double x[2];
+          x[0] = offs[q] * a.scale_d;
+          x[1] = offs[(size_t)ne + q] * a.scale_d;
+          T ph[2][W];
+          int sc[2];
+          if constexpr (DERIV) {
+            T dph[2][W], v[3];
+            sc[0] = kernel_row_d<T, W>(a, x[0], ph[0], dph[0]);
+            sc[1] = kernel_row_d<T, W>(a, x[1], ph[1], dph[1]);
+            interp_grad_cells<T, 2, W>(B, LinIdx<2, W>(gw, sc), ph, dph, v);
+            outs[(size_t)id * ne + q] += (double)v[0];
+            if (nc > 1) {
+              outs[((size_t)1 * p.nd + id) * ne + q] += (double)v[1];
+              outs[((size_t)2 * p.nd + id) * ne + q] += (double)v[2];
+            }
+          } else {
+            sc[0] = kernel_row<T, W>(a, x[0], ph[0]);
+            sc[1] = kernel_row<T, W>(a, x[1], ph[1]);
+            outs[(size_t)id * ne + q] += (double)interp_cells<T, 2, W>(B, LinIdx<2, W>(gw, sc), ph);
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// First entry of a list sorted by k_lpt_keys (ascending keys = descending
+// point counts) whose box holds at most `limit` points.
+__global__ void k_first_at_most_e(const uint64_t* __restrict__ keys, int n, int limit,
+                                  int* __restrict__ out) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    constexpr uint64_t MAXC = (1ull << (LPT_BITS - 1)) - 1;
+    const uint64_t v = MAXC - (uint64_t)limit;  // count <= limit  <=>  key >= v
+    int lo = 0, hi = n;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (keys[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    *out = lo;
+  }
+}
+
 // box partition by evaluation-point count
 __global__ void k_eval_split(int n_eval, const int* __restrict__ eval_box, const int* __restrict__ lo0,
                              const int* __restrict__ hi0, const int* __restrict__ lo1,
@@ -611,6 +711,41 @@ int launch_eval_k(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t
   }
   FGT_LAUNCH_CHECK();
   return 1;
+}
+
+template <typename T>
+int small2_eval_warps(const Geo& g, size_t& smem) {
+  const Small2Layout lay = small2_layout(g.G, g.K);
+  const size_t fix = tw_bytes16<T>(g.G, g.K);
+  const size_t per = sizeof(T) * (size_t)lay.per_warp;
+  if (fix + per > (size_t)MAXSMEM) return 0;
+  const int nw = (int)std::min<size_t>(8, ((size_t)MAXSMEM - fix) / per);
+  smem = fix + per * nw;
+  return nw;
+}
+template <typename T, int W, bool DERIV>
+void launch_eval_small2(PWArgs<T>& a, const EvalPtrs<T>& ep, const int* first, int* next,
+                        cudaStream_t s) {
+  size_t smem = 0;
+  const int nw = small2_eval_warps<T>(a.g, smem);
+  auto k = k_eval_small2<T, W, DERIV>;
+  set_smem(k, smem);
+  k<<<kSMs * std::max(1, 8 / nw), 32 * nw, smem, s>>>(a, ep, first, next);
+  FGT_LAUNCH_CHECK();
+}
+template <typename T>
+void eval_small2_w(int w, bool deriv, PWArgs<T>& a, const EvalPtrs<T>& ep, const int* first,
+                   int* next, cudaStream_t s) {
+#define FGT_S2(WW)                                                              \
+  case WW:                                                                      \
+    if (deriv) launch_eval_small2<T, WW, true>(a, ep, first, next, s);          \
+    else launch_eval_small2<T, WW, false>(a, ep, first, next, s);               \
+    return;
+  switch (w) {
+    FGT_S2(6) FGT_S2(7) FGT_S2(8) FGT_S2(9) FGT_S2(10) FGT_S2(12) FGT_S2(14) FGT_S2(16)
+    default: FGT_REQUIRE(false, FGT_ERR_UNSUPPORTED, "no evaluation kernel for this width");
+  }
+#undef FGT_S2
 }
 
 // deriv: gradients through the kernel derivative (widths 8..16 only)
@@ -727,6 +862,7 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   ep.n_items = nullptr;
   ep.max_items = 0;
   ItemList il;
+  DBuf<int> first2(1, s), next2(1, s);
   DBuf<T> gs;
   {
     // longest-processing-time order of the grid boxes (by point count)
@@ -744,15 +880,30 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
     ep.nbox = L.n_eval;
     ep.nbox_dev = counts.get();
     ep.next = next;
+    // 2D: grid boxes with at most SMALL2_MAX points (a suffix of the order)
+    // go to the warp-per-box kernel, the rest to the CTA kernel
+    size_t sm2 = 0;
+    const bool small2 = P.dim == 2 && !a.g.wrap && (deriv || ep.ncomp_max == 1) &&
+                        small2_eval_warps<T>(a.g, sm2) > 0;
+    if (small2) {
+      next2.zero();
+      k_first_at_most_e<<<1, 32, 0, s>>>(okey, L.n_eval, SMALL2_MAX, first2);
+      FGT_LAUNCH_CHECK();
+    }
     // boxes above the split threshold become several items
     const long long npts = (u0 ? (long long)e0.n : 0) + (u1 ? (long long)e1.n : 0);
-    build_items(il, L.n_eval, counts.get(), reinterpret_cast<const uint32_t*>(lbig.get()),
+    build_items(il, L.n_eval, small2 ? first2.get() : counts.get(),
+                reinterpret_cast<const uint32_t*>(lbig.get()),
                 L.eval_box, u0 ? e0.lo : e1.lo, u0 ? e0.hi : e1.hi, (u0 && u1) ? e1.lo : nullptr,
                 (u0 && u1) ? e1.hi : nullptr, npts, eval_split_threshold(npts), false, s);
     ep.items = il.items;
     ep.n_items = il.n_items;
     ep.max_items = il.max_items;
     launches += 6 + eval_dim<T>(P.dim, Pe.w, a, ep, deriv, gs, s);
+    if (small2) {
+      eval_small2_w<T>(Pe.w, deriv, a, ep, first2, next2, s);
+      launches += 2;
+    }
   }
   {
     ep.boxes = lsmall;

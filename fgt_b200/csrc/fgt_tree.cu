@@ -101,6 +101,26 @@ __global__ void k_box_counts(const uint64_t* __restrict__ bk, int nb, int shift,
   }
 }
 
+// Source count of each box of level l from the exclusive prefix sums S of
+// the per-cell source counts of the full key space (2^(dim*D) cells):
+// count = S[(key+1) << shift] - S[key << shift].
+__global__ void k_box_counts_dense(const uint64_t* __restrict__ bk, int nb, int shift,
+                                   const int* __restrict__ S, int* __restrict__ cnt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+    cnt[i] = S[(bk[i] + 1) << shift] - S[bk[i] << shift];
+}
+
+// Per-cell source counts of the full key space; lanes of a warp that hit
+// the same cell add once (points arrive in input order, often clustered).
+__global__ void k_cell_hist(const uint64_t* __restrict__ keys, int n, int* __restrict__ h) {
+  for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+    const int i = i0 + threadIdx.x;
+    const unsigned long long k = i < n ? keys[i] : ~0ull;
+    const unsigned peers = __match_any_sync(0xffffffffu, k);
+    if (i < n && (__ffs(peers) - 1) == (int)(threadIdx.x & 31)) atomicAdd(&h[k], __popc(peers));
+  }
+}
+
 __global__ void k_flag_gt(const int* __restrict__ cnt, int n, int ndiv, int* __restrict__ f) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     f[i] = cnt[i] > ndiv ? 1 : 0;
@@ -202,16 +222,37 @@ __global__ void k_leaf_flags(const int* __restrict__ nonleaf, int n, int* __rest
 }
 __global__ void k_leaf_starts(const uint64_t* __restrict__ key, const int* __restrict__ level,
                               const int* __restrict__ f, const int* __restrict__ pos, int n,
-                              int dim, int D, uint64_t* __restrict__ ls) {
+                              int dim, int D, uint64_t* __restrict__ ls,
+                              uint32_t* __restrict__ lbox) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    if (f[i]) ls[pos[i]] = key[i] << (dim * (D - level[i]));
+    if (f[i]) {
+      ls[pos[i]] = key[i] << (dim * (D - level[i]));
+      lbox[pos[i]] = (uint32_t)i;
+    }
+}
+
+// Reference box of every leaf (by leaf ordinal): the leaf itself when it
+// lies at or above the cut-off level, else its ancestor at that level.
+__global__ void k_leaf_ref(const uint32_t* __restrict__ lbox, int nl, const int* __restrict__ level,
+                           const int* __restrict__ parent, int ncutoff, int* __restrict__ lref) {
+  for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < nl; o += gridDim.x * blockDim.x) {
+    int b = (int)lbox[o];
+    while (level[b] > ncutoff) b = parent[b];
+    lref[o] = b;
+  }
+}
+// ref[p] = lref[ordinal of sorted point p]
+__global__ void k_point_ref(const uint32_t* __restrict__ ord, int n, const int* __restrict__ lref,
+                            int* __restrict__ ref) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    ref[i] = lref[ord[i]];
 }
 
 // Leaf ordinal of each point (upper_bound - 1 over sorted leaf start keys);
 // doubles as the radix key, the value is the original index.
 __global__ void k_point_leaf(const uint64_t* __restrict__ pk, int n,
                              const uint64_t* __restrict__ ls, int nl,
-                             uint64_t* __restrict__ ord, uint32_t* __restrict__ idx) {
+                             uint32_t* __restrict__ ord, uint32_t* __restrict__ idx) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint64_t v = pk[i];
     int lo = 0, hi = nl;  // first start > v
@@ -219,19 +260,19 @@ __global__ void k_point_leaf(const uint64_t* __restrict__ pk, int n,
       int mid = (lo + hi) >> 1;
       if (ls[mid] <= v) lo = mid + 1; else hi = mid;
     }
-    ord[i] = (uint64_t)(lo - 1);
+    ord[i] = (uint32_t)(lo - 1);
     idx[i] = (uint32_t)i;
   }
 }
 
 // leaf_lo[o] = first sorted position with ordinal >= o, o = 0..nl
-__global__ void k_leaf_point_lo(const uint64_t* __restrict__ ord, int n, int nl,
+__global__ void k_leaf_point_lo(const uint32_t* __restrict__ ord, int n, int nl,
                                 int* __restrict__ lo) {
   for (int o = blockIdx.x * blockDim.x + threadIdx.x; o <= nl; o += gridDim.x * blockDim.x) {
     int a = 0, b = n;
     while (a < b) {
       int m = (a + b) >> 1;
-      if (ord[m] < (uint64_t)o) a = m + 1; else b = m;
+      if (ord[m] < (uint32_t)o) a = m + 1; else b = m;
     }
     lo[o] = a;
   }
@@ -248,18 +289,6 @@ __global__ void k_box_ranges(const uint64_t* __restrict__ key, const int* __rest
     int a = dev_lower_bound(ls, nl, lo), c = dev_lower_bound(ls, nl, hi);
     s0[b] = slo[a]; s1[b] = slo[c];
     t0[b] = tlo[a]; t1[b] = tlo[c];
-  }
-}
-
-// Reference box of every sorted point: its box at level ncutoff, or its leaf
-// when the leaf is coarser.
-__global__ void k_ref_boxes(const int* __restrict__ level, const int* __restrict__ nonleaf,
-                            int nboxes, int ncutoff, const int* __restrict__ lo,
-                            const int* __restrict__ hi, int* __restrict__ ref) {
-  for (int b = blockIdx.x; b < nboxes; b += gridDim.x) {
-    int l = level[b];
-    if (l == ncutoff || (l < ncutoff && !nonleaf[b]))
-      for (int p = lo[b] + threadIdx.x; p < hi[b]; p += blockDim.x) ref[p] = b;
   }
 }
 
@@ -342,13 +371,30 @@ void tree_build(Tree& t, int dim, int iperiod, int npwlevel, int ndiv, double bs
     }
   }
   // 1. full keys of sources and targets
-  DBuf<uint64_t> skey(ns, s), tkey(nt, s), ksorted(ns, s), ktmp(std::max(ns, nt), s);
+  DBuf<uint64_t> skey(ns, s), tkey(nt, s), ksorted, ktmp(std::max(ns, nt), s);
   if (ns > 0) launch_point_keys(dim, d_src, ns, kp, skey, s);
   if (nt > 0) launch_point_keys(dim, d_trg, nt, kp, tkey, s);
-  if (ns > 0)
-    FGT_CUDA(cudaMemcpyAsync(ksorted.get(), skey.get(), sizeof(uint64_t) * ns,
-                             cudaMemcpyDeviceToDevice, s));
-  radix_sort(ksorted, nullptr, ktmp, nullptr, ns, dim * D, s);
+  // Source counts per box come from a dense histogram of the full keys
+  // (prefix sums over the 2^(dim*D) finest cells) when the key space is
+  // small enough, else from binary searches in the sorted keys.
+  const bool dense = dim * D <= 24;
+  DBuf<int> cellsum;
+  if (dense) {
+    const int ncell = 1 << (dim * D);
+    cellsum.alloc((size_t)ncell + 1, s);
+    cellsum.zero();
+    if (ns > 0) {
+      k_cell_hist<<<grid_for(ns, 256), 256, 0, s>>>(skey, ns, cellsum);
+      FGT_LAUNCH_CHECK();
+    }
+    exclusive_scan_i32(cellsum, cellsum, ncell + 1, nullptr, s);
+  } else {
+    ksorted.alloc(std::max(ns, 1), s);
+    if (ns > 0)
+      FGT_CUDA(cudaMemcpyAsync(ksorted.get(), skey.get(), sizeof(uint64_t) * ns,
+                               cudaMemcpyDeviceToDevice, s));
+    radix_sort(ksorted, nullptr, ktmp, nullptr, ns, dim * D, s);
+  }
 
   // 2. refinement on source counts (pts_tree_build, pts_tree_nd.f:520-590)
   std::vector<DBuf<uint64_t>> lk;   // keys of each level
@@ -361,7 +407,10 @@ void tree_build(Tree& t, int dim, int iperiod, int npwlevel, int ndiv, double bs
   for (int l = 0; l < D; l++) {
     int nb = nlk[l];
     DBuf<int> cnt(nb, s), flag(nb, s), pos(nb, s), tot(1, s);
-    k_box_counts<<<grid_for(nb, 256), 256, 0, s>>>(lk[l], nb, dim * (D - l), ksorted, ns, cnt);
+    if (dense)
+      k_box_counts_dense<<<grid_for(nb, 256), 256, 0, s>>>(lk[l], nb, dim * (D - l), cellsum, cnt);
+    else
+      k_box_counts<<<grid_for(nb, 256), 256, 0, s>>>(lk[l], nb, dim * (D - l), ksorted, ns, cnt);
     FGT_LAUNCH_CHECK();
     k_flag_gt<<<grid_for(nb, 256), 256, 0, s>>>(cnt, nb, ndiv, flag);
     FGT_LAUNCH_CHECK();
@@ -457,32 +506,48 @@ void tree_build(Tree& t, int dim, int iperiod, int npwlevel, int ndiv, double bs
   int nl = fetch_int(ltot, s);
   t.nleaves = nl;
   DBuf<uint64_t> ls(nl, s), lstmp(nl, s);
+  DBuf<uint32_t> lbox(nl, s), lbtmp(nl, s);
   k_leaf_starts<<<grid_for(nboxes, 256), 256, 0, s>>>(t.key, t.level, lf, lpos, nboxes, dim, D,
-                                                       ls);
+                                                       ls, lbox);
   FGT_LAUNCH_CHECK();
-  radix_sort(ls, nullptr, lstmp, nullptr, nl, dim * D, s);
+  radix_sort(ls, lbox, lstmp, lbtmp, nl, dim * D, s);
+  DBuf<int> lref(std::max(nl, 1), s);
+  k_leaf_ref<<<grid_for(nl, 256), 256, 0, s>>>(lbox, nl, t.level, t.parent, t.ncutoff, lref);
+  FGT_LAUNCH_CHECK();
   int obits = bits_for(nl);
   DBuf<int> slo(nl + 1, s), tlo(nl + 1, s);
+  t.src_ref.alloc(std::max(ns, 1), s);
+  t.trg_ref.alloc(std::max(nt, 1), s);
   {
-    DBuf<uint64_t> ord(std::max(ns, 1), s);
+    // leaf ordinals as 32-bit keys (half the key traffic of the sort)
+    DBuf<uint32_t> ord(std::max(ns, 1), s);
     DBuf<uint32_t> vtmp(std::max(std::max(ns, nt), 1), s);
+    uint32_t* otmp = reinterpret_cast<uint32_t*>(ktmp.get());  // >= max(ns, nt) u32
     t.isrc.alloc(std::max(ns, 1), s);
     if (ns > 0) {
       k_point_leaf<<<grid_for(ns, 256), 256, 0, s>>>(skey, ns, ls, nl, ord, t.isrc);
       FGT_LAUNCH_CHECK();
-      radix_sort(ord, t.isrc, ktmp, vtmp, ns, obits, s);
+      radix_sort_u32(ord, t.isrc, otmp, vtmp, ns, obits, s);
     }
     k_leaf_point_lo<<<grid_for(nl + 1, 256), 256, 0, s>>>(ord, ns, nl, slo);
     FGT_LAUNCH_CHECK();
-    DBuf<uint64_t> tord(std::max(nt, 1), s);
+    if (ns > 0) {
+      k_point_ref<<<grid_for(ns, 256), 256, 0, s>>>(ord, ns, lref, t.src_ref);
+      FGT_LAUNCH_CHECK();
+    }
+    DBuf<uint32_t> tord(std::max(nt, 1), s);
     t.itrg.alloc(std::max(nt, 1), s);
     if (nt > 0) {
       k_point_leaf<<<grid_for(nt, 256), 256, 0, s>>>(tkey, nt, ls, nl, tord, t.itrg);
       FGT_LAUNCH_CHECK();
-      radix_sort(tord, t.itrg, ktmp, vtmp, nt, obits, s);
+      radix_sort_u32(tord, t.itrg, otmp, vtmp, nt, obits, s);
     }
     k_leaf_point_lo<<<grid_for(nl + 1, 256), 256, 0, s>>>(tord, nt, nl, tlo);
     FGT_LAUNCH_CHECK();
+    if (nt > 0) {
+      k_point_ref<<<grid_for(nt, 256), 256, 0, s>>>(tord, nt, lref, t.trg_ref);
+      FGT_LAUNCH_CHECK();
+    }
   }
   t.src_lo.alloc(nboxes, s);
   t.src_hi.alloc(nboxes, s);
@@ -491,15 +556,6 @@ void tree_build(Tree& t, int dim, int iperiod, int npwlevel, int ndiv, double bs
   k_box_ranges<<<grid_for(nboxes, 256), 256, 0, s>>>(t.key, t.level, nboxes, dim, D, ls, nl, slo,
                                                       tlo, t.src_lo, t.src_hi, t.trg_lo,
                                                       t.trg_hi);
-  FGT_LAUNCH_CHECK();
-  t.src_ref.alloc(std::max(ns, 1), s);
-  t.trg_ref.alloc(std::max(nt, 1), s);
-  int gb = std::min(nboxes, 8 * kSMs * 4);
-  k_ref_boxes<<<gb, 128, 0, s>>>(t.level, t.nonleaf, nboxes, t.ncutoff, t.src_lo, t.src_hi,
-                                 t.src_ref);
-  FGT_LAUNCH_CHECK();
-  k_ref_boxes<<<gb, 128, 0, s>>>(t.level, t.nonleaf, nboxes, t.ncutoff, t.trg_lo, t.trg_hi,
-                                 t.trg_ref);
   FGT_LAUNCH_CHECK();
 }
 

@@ -1494,14 +1494,16 @@ void oracle_direct_exact(int nd, int dim, double delta, int iperiod, double bs0,
                          const double *charge, int ifdipole, const double *rnormal,
                          const double *dipstr, int nt, const double *targ, int ifpgh,
                          double *pot, double *grad, double *hess) {
-  int nhess = dim * (dim + 1) / 2, j, i, k;
+  int nhess = dim * (dim + 1) / 2, j;
   int ni = iperiod ? nimg : 0, span = 2 * ni + 1, nimgs = ipow(span, dim);
   memset(pot, 0, sizeof(double) * (size_t)nt * nd);
   if (ifpgh >= 2) memset(grad, 0, sizeof(double) * (size_t)nt * nd * dim);
   if (ifpgh >= 3) memset(hess, 0, sizeof(double) * (size_t)nt * nd * nhess);
+  /* evaluation points are independent (each writes its own outputs) */
+#pragma omp parallel for schedule(dynamic, 1)
   for (j = 0; j < nt; j++)
-    for (i = 0; i < ns; i++) {
-      int im;
+    for (int i = 0; i < ns; i++) {
+      int im, k;
       for (im = 0; im < nimgs; im++) {
         double dr[MAXDIM];
         int r = im;
