@@ -18,6 +18,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfgt_b200.so")
+LIB_CHECK_PATH = os.path.join(_HERE, "libfgt_b200_check.so")  # FGT_CHECK build
 
 FGT_OK = 0
 FGT_ERR_ARG = 1
@@ -27,6 +28,7 @@ FGT_ERR_UNSUPPORTED = 4
 FGT_ERR_TIMEOUT = 5
 FGT_ERR_NODEVICE = 6
 FGT_ERR_INJECTED = 7
+FGT_ERR_CHECK = 8
 
 PREC_AUTO = 0
 PREC_FP64 = 1
@@ -88,17 +90,30 @@ class FgtInstance(C.Structure):
 EXPORTS = ["fgt_opts_default", "fgt_pfgt_c", "pfgt_", "pfgt_direct_", "fgt_last_status",
            "fgt_last_error", "fgt_version", "fgt_debug_tree_build", "fgt_debug_tree_get",
            "fgt_debug_tree_free", "fgt_direct_nomalloc", "fgt_pfgt_batch", "fgt_plan_create",
-           "fgt_plan_execute", "fgt_plan_destroy"]
+           "fgt_plan_execute", "fgt_plan_destroy", "fgt_check_selftest"]
 
 
-def lib():
-    """Load libfgt_b200.so (raises if it is missing: no CPU fallback)."""
+_libs = {}
+
+
+def lib(check=False):
+    """Load libfgt_b200.so, or with check=True the FGT_CHECK build
+    libfgt_b200_check.so (raises if it is missing: no CPU fallback)."""
     global _lib
+    if check:
+        if "check" not in _libs:
+            _libs["check"] = _load(LIB_CHECK_PATH, "python -m fgt_b200.build --check")
+        return _libs["check"]
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise FgtError(FGT_ERR_NODEVICE,
-                           f"{LIB_PATH} not built; run python -m fgt_b200.build")
-        L = C.CDLL(LIB_PATH)
+        _lib = _load(LIB_PATH, "python -m fgt_b200.build")
+    return _lib
+
+
+def _load(path, how):
+    if True:
+        if not os.path.exists(path):
+            raise FgtError(FGT_ERR_NODEVICE, f"{path} not built; run {how}")
+        L = C.CDLL(path)
         L.fgt_pfgt_c.restype = C.c_int
         L.fgt_pfgt_c.argtypes = [
             C.POINTER(FgtOpts), C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _dp, _dp,
@@ -113,16 +128,17 @@ def lib():
         L.fgt_debug_tree_get.restype = C.c_long
         L.fgt_debug_tree_get.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_long]
         L.fgt_debug_tree_free.argtypes = [C.c_void_p]
-        _lib = L
-    return _lib
+        L.fgt_check_selftest.restype = C.c_int
+        L.fgt_check_selftest.argtypes = []
+    return L
 
 
 def version():
     return lib().fgt_version().decode()
 
 
-def last_error():
-    return lib().fgt_last_error().decode()
+def last_error(check=False):
+    return lib(check).fgt_last_error().decode()
 
 
 def _f64(a, shape):
@@ -136,13 +152,14 @@ def _ptr(a):
 
 def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None, rnormal=None,
          ifpgh=1, targets=None, ifpghtarg=0, bs0=1.0, cen0=None, precision=PREC_AUTO,
-         ndiv=0, small_eval=-1, spread_width=0, stats=False, timing=False):
+         ndiv=0, small_eval=-1, spread_width=0, stats=False, timing=False, check=False):
     """Point FGT with the reference's argument meaning (src/pfgt/pfgt.f:11-53).
 
     Returns a dict with pot/grad/hess (sources) and pottarg/gradtarg/hesstarg
     (targets) for the requested levels, plus bs0/cen0 (and stats if asked).
+    check=True runs the FGT_CHECK build (device bounds checks).
     """
-    L = lib()
+    L = lib(check)
     src = _f64(sources, (-1, dim))
     ns = src.shape[0]
     trg = None if targets is None else _f64(targets, (-1, dim))
@@ -177,7 +194,7 @@ def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None, rnorma
                       _ptr(rn), _ptr(ds), ifpgh, _ptr(pot), _ptr(grad), _ptr(hess), nt,
                       _ptr(trg), ifpghtarg if nt else 0, _ptr(pt), _ptr(gt), _ptr(ht))
     if rc != FGT_OK:
-        raise FgtError(rc, last_error())
+        raise FgtError(rc, last_error(check))
     out = {"bs0": b0.value, "cen0": c0[:dim].copy()}
     for k, v in (("pot", pot), ("grad", grad), ("hess", hess), ("pottarg", pt),
                  ("gradtarg", gt), ("hesstarg", ht)):

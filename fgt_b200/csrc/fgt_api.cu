@@ -35,7 +35,8 @@ constexpr int UB = 4;
 template <typename T, int DIM>
 __global__ void k_gather_coords(const double* __restrict__ x, int n,
                                 const uint32_t* __restrict__ perm, const int* __restrict__ ref,
-                                const double* __restrict__ center, T* __restrict__ off) {
+                                const double* __restrict__ center, int nboxes,
+                                T* __restrict__ off) {
   const int st = gridDim.x * blockDim.x;
   for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += UB * st) {
     size_t o[UB];
@@ -45,6 +46,8 @@ __global__ void k_gather_coords(const double* __restrict__ x, int n,
       const int i = i0 + u * st;
       o[u] = i < n ? perm[i] : 0;
       b[u] = i < n ? ref[i] : 0;
+      if (!FGT_DCHECK(o[u] < (size_t)n, 101)) o[u] = 0;
+      if (!FGT_DCHECK(b[u] >= 0 && b[u] < nboxes, 102)) b[u] = 0;
     }
     double v[UB][DIM], c[UB][DIM];
 #pragma unroll
@@ -66,11 +69,11 @@ __global__ void k_gather_coords(const double* __restrict__ x, int n,
 }
 template <typename T>
 void launch_gather_coords(int dim, const double* x, int n, const uint32_t* perm, const int* ref,
-                          const double* center, T* off, cudaStream_t s) {
+                          const double* center, int nboxes, T* off, cudaStream_t s) {
   const int grid = grid_for(n, 256);
-  if (dim == 1) k_gather_coords<T, 1><<<grid, 256, 0, s>>>(x, n, perm, ref, center, off);
-  else if (dim == 2) k_gather_coords<T, 2><<<grid, 256, 0, s>>>(x, n, perm, ref, center, off);
-  else k_gather_coords<T, 3><<<grid, 256, 0, s>>>(x, n, perm, ref, center, off);
+  if (dim == 1) k_gather_coords<T, 1><<<grid, 256, 0, s>>>(x, n, perm, ref, center, nboxes, off);
+  else if (dim == 2) k_gather_coords<T, 2><<<grid, 256, 0, s>>>(x, n, perm, ref, center, nboxes, off);
+  else k_gather_coords<T, 3><<<grid, 256, 0, s>>>(x, n, perm, ref, center, nboxes, off);
   FGT_LAUNCH_CHECK();
 }
 
@@ -79,6 +82,7 @@ __global__ void k_gather_vals(const double* __restrict__ v, int n, int nv,
                               const uint32_t* __restrict__ perm, T* __restrict__ out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     size_t o = perm[i];
+    if (!FGT_DCHECK(o < (size_t)n, 103)) continue;
     for (int j = 0; j < nv; j++) out[(size_t)j * n + i] = (T)v[o * nv + j];
   }
 }
@@ -86,7 +90,7 @@ __global__ void k_gather_vals(const double* __restrict__ v, int n, int nv,
 // inv[perm[i]] = i
 __global__ void k_invert(const uint32_t* __restrict__ perm, int n, uint32_t* __restrict__ inv) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    inv[perm[i]] = (uint32_t)i;
+    if (FGT_DCHECK(perm[i] < (uint32_t)n, 104)) inv[perm[i]] = (uint32_t)i;
 }
 
 // out[o] = sorted[inv[o]] for pot/grad/hess in the reference's layouts
@@ -101,7 +105,10 @@ __global__ void k_gather_out(const double* __restrict__ srt, int n, int nd, int 
   for (int o0 = blockIdx.x * blockDim.x + threadIdx.x; o0 < n; o0 += UB * st) {
     size_t iu[UB];
 #pragma unroll
-    for (int u = 0; u < UB; u++) iu[u] = o0 + u * st < n ? inv[o0 + u * st] : 0;
+    for (int u = 0; u < UB; u++) {
+      iu[u] = o0 + u * st < n ? inv[o0 + u * st] : 0;
+      if (!FGT_DCHECK(iu[u] < (size_t)n, 105)) iu[u] = 0;
+    }
     for (int id = 0; id < nd; id++) {
       double v[UB];
 #pragma unroll
@@ -382,10 +389,10 @@ void setup_geometry(Setup& u, const Call& c, double* bs0_io, double* cen0_io, co
   // --- gather (dreorderf, fmmcommon2d.f:3-27) as offsets from reference boxes
   u.soff.alloc((size_t)c.ns * dim, s);
   u.toff.alloc((size_t)std::max(c.nt, 1) * dim, s);
-  launch_gather_coords<double>(dim, c.src, c.ns, t.isrc, t.src_ref, t.center, u.soff, s);
+  launch_gather_coords<double>(dim, c.src, c.ns, t.isrc, t.src_ref, t.center, t.nboxes, u.soff, s);
   launches++;
   if (c.nt > 0) {
-    launch_gather_coords<double>(dim, c.trg, c.nt, t.itrg, t.trg_ref, t.center, u.toff, s);
+    launch_gather_coords<double>(dim, c.trg, c.nt, t.itrg, t.trg_ref, t.center, t.nboxes, u.toff, s);
     launches++;
   }
   // inverse leaf permutations for the output reorder
@@ -575,6 +582,22 @@ bool fault_requested(const char* what) {
   return f && strstr(f, what) != nullptr;
 }
 
+// FGT_CHECK build: fail the call when any device bounds check fired during
+// it (the first failing site is named); nothing in the normal build.
+void raise_failed_checks(cudaStream_t s) {
+#ifdef FGT_CHECK
+  const unsigned site = check_sites(s);
+  if (site) {
+    static thread_local char msg[96];
+    snprintf(msg, sizeof(msg), "device bounds check failed at site %u", site);
+    fgt_set_error_message(msg, __FILE__, __LINE__);
+    throw Error{FGT_ERR_CHECK, msg};
+  }
+#else
+  (void)s;
+#endif
+}
+
 int pfgt_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps, int iperiod,
               double* bs0, double* cen0, int ns, const double* sources, int ifcharge,
               const double* charge, int ifdipole, const double* rnormal, const double* dipstr,
@@ -704,6 +727,7 @@ int pfgt_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps
   }
   tm.mark(9);
   FGT_CUDA(cudaStreamSynchronize(s));
+  raise_failed_checks(s);
   if (st) {
     st->precision_used = prec;
     tm.finish(st->ms);
@@ -867,6 +891,7 @@ int plan_execute_impl(fgt_plan* pl, int ifcharge, const double* charge, int ifdi
     if (pght >= 3) d2h(hesstarg, d_ht, (size_t)nt * nd * nhess);
   }
   FGT_CUDA(cudaStreamSynchronize(s));
+  raise_failed_checks(s);
   return FGT_OK;
 }
 
@@ -1139,9 +1164,50 @@ extern "C" void pfgt_direct_(const int* nd, const int* dim, const double* delta,
       if (dg) FGT_CUDA(cudaMemcpyAsync(grad + (size_t)js * n * d, dg, sizeof(double) * nt * n * d, cudaMemcpyDeviceToHost, s));
       if (dh) FGT_CUDA(cudaMemcpyAsync(hess + (size_t)js * n * nh, dh, sizeof(double) * nt * n * nh, cudaMemcpyDeviceToHost, s));
       FGT_CUDA(cudaStreamSynchronize(s));
+      raise_failed_checks(s);
     }
   } catch (const fgt::Error& e) {
     st = e.code;
   }
   g_last_status = st;
+}
+
+// ---------------------------------------------------------------------------
+// Self-test of the FGT_CHECK build: the strength gather with a host-crafted
+// permutation whose third entry points past the array.  The checked kernel
+// records the failure and skips that element; the call then reports
+// FGT_ERR_CHECK.  The normal build has no checks: FGT_ERR_UNSUPPORTED.
+extern "C" int fgt_check_selftest(void) {
+  using namespace fgt;
+  int st = FGT_OK;
+  try {
+#ifndef FGT_CHECK
+    FGT_REQUIRE(false, FGT_ERR_UNSUPPORTED, "library built without FGT_CHECK");
+#else
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      (void)cudaGetLastError();
+      throw Error{FGT_ERR_NODEVICE, "no CUDA device"};
+    }
+    int dev = 0;
+    FGT_CUDA(cudaGetDevice(&dev));
+    cudaStream_t s = library_stream(dev);
+    ArenaScope arena_scope(s);
+    const int n = 4;
+    const uint32_t hperm[n] = {0, 1, n + 5, 2};  // entry 2 is out of range
+    const double hv[n] = {1, 2, 3, 4};
+    DBuf<uint32_t> perm(n, s);
+    DBuf<double> v(n, s), out(n, s);
+    FGT_CUDA(cudaMemcpyAsync(perm.get(), hperm, sizeof(hperm), cudaMemcpyHostToDevice, s));
+    FGT_CUDA(cudaMemcpyAsync(v.get(), hv, sizeof(hv), cudaMemcpyHostToDevice, s));
+    k_gather_vals<double><<<1, 32, 0, s>>>(v, n, 1, perm, out);
+    FGT_LAUNCH_CHECK();
+    FGT_CUDA(cudaStreamSynchronize(s));
+    raise_failed_checks(s);
+#endif
+  } catch (const fgt::Error& e) {
+    st = e.code;
+  }
+  g_last_status = st;
+  return st;
 }

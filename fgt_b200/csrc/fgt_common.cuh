@@ -39,6 +39,49 @@ struct Error {
 
 extern "C" void fgt_set_error_message(const char* msg, const char* file, int line);
 
+// Device bounds checks of the FGT_CHECK build (the stand-in for a memory
+// checker): FGT_DCHECK(cond, site) is true when cond holds; otherwise it
+// records `site` in the module's check word (first failure wins) and is
+// false, so the caller skips the access.  Never traps.  The host reads and
+// clears every module's word at the end of a call (check_sites) and fails the
+// call with FGT_ERR_CHECK.  In the normal build the macro is the constant
+// true and costs nothing.
+namespace fgt {
+using CheckReader = unsigned (*)(cudaStream_t);
+void register_check_reader(CheckReader r);
+// First failed check site of any module since the last call (0 = none);
+// clears the words.  Synchronises the stream.
+unsigned check_sites(cudaStream_t s);
+}  // namespace fgt
+#ifdef FGT_CHECK
+namespace fgt {
+namespace {
+__device__ unsigned int g_check_site;
+unsigned read_check_site(cudaStream_t s) {
+  unsigned v = 0, z = 0;
+  if (cudaMemcpyFromSymbolAsync(&v, g_check_site, sizeof(v), 0, cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0xffffffffu;
+  }
+  if (v && cudaMemcpyToSymbolAsync(g_check_site, &z, sizeof(z), 0, cudaMemcpyHostToDevice, s) !=
+               cudaSuccess)
+    (void)cudaGetLastError();
+  return v;
+}
+struct CheckRegistrar {
+  CheckRegistrar() { register_check_reader(read_check_site); }
+};
+CheckRegistrar check_registrar;
+}  // namespace
+}  // namespace fgt
+#define FGT_DCHECK(cond, site) \
+  ((cond) || (atomicCAS(&fgt::g_check_site, 0u, (unsigned)(site)), false))
+#else
+#define FGT_DCHECK(cond, site) (true)
+#endif
+
 namespace fgt {
 
 constexpr int kSMs = 148;

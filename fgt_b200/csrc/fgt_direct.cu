@@ -16,6 +16,7 @@ constexpr int DW = 4;  // warps per block
 template <typename T>
 struct DArgs {
   int n_items, nd, d0, ne, ns, iperiod0;  // n_items: upper bound
+  int nboxes;
   const int* n_items_dev;                  // item count on the device
   T dinv, dmax, rfac;  // 1/delta, cut-off, 2/delta
   double bs0;
@@ -104,6 +105,7 @@ __global__ void __launch_bounds__(DW * 32) k_direct(DArgs<T> a) {
     const int lT = a.level[tb];
     for (int li = a.l1_ptr[tb]; li < a.l1_ptr[tb + 1]; li++) {
       const int sb = a.l1_src[li];
+      if (!FGT_DCHECK(sb >= 0 && sb < a.nboxes, 401)) continue;
       double dc[DIM];
 #pragma unroll
       for (int k = 0; k < DIM; k++) {
@@ -276,6 +278,7 @@ __global__ void __launch_bounds__(DW * 32) k_direct32(DArgs<float> a) {
     const int lT = a.level[tb];
     for (int li = a.l1_ptr[tb]; li < a.l1_ptr[tb + 1]; li++) {
       const int sb = a.l1_src[li];
+      if (!FGT_DCHECK(sb >= 0 && sb < a.nboxes, 401)) continue;
       double dc[DIM];
 #pragma unroll
       for (int k = 0; k < DIM; k++) {
@@ -463,6 +466,7 @@ __global__ void __launch_bounds__(DW * 32) k_direct32x2(DArgs<float> a) {
     const int lT = a.level[tb];
     for (int li = a.l1_ptr[tb]; li < a.l1_ptr[tb + 1]; li++) {
       const int sbx = a.l1_src[li];
+      if (!FGT_DCHECK(sbx >= 0 && sbx < a.nboxes, 402)) continue;
       double dc[DIM];
 #pragma unroll
       for (int k = 0; k < DIM; k++) {
@@ -577,6 +581,7 @@ __global__ void k_near_lists(NearArgs n) {
     for (int li = e0; li < e1; li++) {
       int kept = 0;
       const int sbx = n.l1_src[li];
+      if (!FGT_DCHECK(sbx >= 0 && sbx < n.nboxes, 403)) continue;
       double dc[DIM];
 #pragma unroll
       for (int k = 0; k < DIM; k++) {
@@ -926,6 +931,7 @@ int direct_near_field(const DirectGeom& g, const Lists& L, const SourceSet<T>& s
   a.ne = e.n;
   a.ns = src.n;
   a.iperiod0 = g.iperiod0;
+  a.nboxes = g.nboxes;
   a.dinv = (T)(1.0 / g.delta);
   a.dmax = (T)g.dmax;
   a.rfac = (T)(2.0 / g.delta);

@@ -245,9 +245,11 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
     if (s_next >= n_items) break;
     const WorkItem it = io.items[s_next];
     const int fb = it.slot;
+    if (!FGT_DCHECK(fb >= 0 && fb < io.n_form, 201)) continue;
     const int box = io.form_box[fb];
     int p0, p1;
     part_range(io.s_lo[box], io.s_hi[box], it.part, it.nparts, p0, p1);
+    if (!FGT_DCHECK(p0 >= 0 && p0 <= p1 && p1 <= io.ns, 202)) continue;
     T* mp_base = it.pslot >= 0 ? p.partial + (size_t)it.pslot * io.nd * 2 * g.nexp
                                : p.mp + (size_t)fb * io.nd * 2 * g.nexp;
     for (int id = 0; id < io.nd; id++) {
@@ -375,8 +377,10 @@ __global__ void __launch_bounds__(256) k_form_small2(PWArgs<T> a, FormIO io, For
     bi = __shfl_sync(0xffffffffu, bi, 0) + f0;
     if (bi >= io.n_form) break;
     const int fb = (int)order[bi];
+    if (!FGT_DCHECK(fb >= 0 && fb < io.n_form, 203)) continue;
     const int box = io.form_box[fb];
     const int p0 = io.s_lo[box], p1 = io.s_hi[box];
+    if (!FGT_DCHECK(p0 >= 0 && p0 <= p1 && p1 <= io.ns && p1 - p0 <= SMALL2_MAX, 204)) continue;
     for (int id = 0; id < io.nd; id++) {
       T* mp = p.mp + ((size_t)fb * io.nd + id) * 2 * g.nexp;
       for (int comp = 0; comp < io.ncomp; comp++) {
@@ -499,7 +503,8 @@ constexpr int TRANS_MPT = 4;
 // src/pfgt/bfgt_pwrouts.f:1555-1636), one mode per thread, complex values
 // as 8- or 16-byte vectors.
 template <typename T>
-__global__ void k_translate(int n_eval, int nexp, int nd, int ge, const int* __restrict__ self,
+__global__ void k_translate(int n_eval, int n_form, int nsh, int nexp, int nd, int ge,
+                            const int* __restrict__ self,
                             const int* __restrict__ ptr, const int* __restrict__ src,
                             const int* __restrict__ widx, const T* __restrict__ mp,
                             const T* __restrict__ wtab, T* __restrict__ loc) {
@@ -525,6 +530,8 @@ __global__ void k_translate(int n_eval, int nexp, int nd, int ge, const int* __r
         if (sf >= 0 && ok[i]) acc[i] = __ldg(sp + i * blockDim.x);
       }
       for (int j = j0; j < j1; j++) {
+        if (!FGT_DCHECK(src[j] >= 0 && src[j] < n_form && widx[j] >= 0 && widx[j] < nsh, 205))
+          continue;
         const V* ap = mpv + ((size_t)src[j] * nd + id) * nexp + m0;
         const V* wp = wv + (size_t)widx[j] * nexp + m0;
         V av[MPT], w[MPT];
@@ -905,7 +912,7 @@ int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, PWWork* work, 
   for (int e0 = 0; e0 < L.n_eval; e0 += 65535 * TGE) {
     int ne = std::min(65535 * TGE, L.n_eval - e0);
     dim3 grid(gx, ceil_div(ne, TGE));
-    k_translate<T><<<grid, 256, 0, s>>>(ne, P.nexp, P.nd, TGE, L.eval_self.get() + e0,
+    k_translate<T><<<grid, 256, 0, s>>>(ne, L.n_form, nsh, P.nexp, P.nd, TGE, L.eval_self.get() + e0,
                                         L.trans_ptr.get() + e0, L.trans_src, L.trans_w, D.mp,
                                         D.wtab, D.loc.get() + (size_t)e0 * P.nd * 2 * P.nexp);
     FGT_LAUNCH_CHECK();

@@ -174,6 +174,7 @@ __global__ void __launch_bounds__(eval_threads<T, DIM, W, GB, DERIV>())
     if (bi >= n_items) break;
     const WorkItem it = p.items[bi];
     const int e = it.slot;
+    if (!FGT_DCHECK(e >= 0 && e < p.nbox, 301)) continue;
     const int box = p.eval_box[e];
     for (int id = 0; id < p.nd; id++) {
       const T* L = p.loc + ((size_t)e * p.nd + id) * 2 * g.nexp;
@@ -189,6 +190,7 @@ __global__ void __launch_bounds__(eval_threads<T, DIM, W, GB, DERIV>())
           int q0, q1;
           part_range(set ? p.lo[1][box] : p.lo[0][box], set ? p.hi[1][box] : p.hi[0][box],
                      it.part, it.nparts, q0, q1);
+          if (!FGT_DCHECK(q0 >= 0 && q0 <= q1 && q1 <= ne, 302)) continue;
           for (int c0 = q0; c0 < q1; c0 += ORDER_CHUNK) {
             const int n = min(ORDER_CHUNK, q1 - c0);
             if (p.cell_bins > 0)
@@ -584,6 +586,7 @@ __global__ void __launch_bounds__(256) k_eval_small2(PWArgs<T> a, EvalPtrs<T> p,
     bi = __shfl_sync(0xffffffffu, bi, 0) + f0;
     if (bi >= nbox) break;
     const int e = p.boxes[bi];
+    if (!FGT_DCHECK(e >= 0 && e < p.nbox, 303)) continue;
     const int box = p.eval_box[e];
     for (int id = 0; id < p.nd; id++) {
       const T* L = p.loc + ((size_t)e * p.nd + id) * 2 * g.nexp;
@@ -610,6 +613,7 @@ __global__ void __launch_bounds__(256) k_eval_small2(PWArgs<T> a, EvalPtrs<T> p,
         double* outs = set ? p.out[1] : p.out[0];
         const int q0 = set ? p.lo[1][box] : p.lo[0][box];
         const int q1 = set ? p.hi[1][box] : p.hi[0][box];
+        if (!FGT_DCHECK(q0 >= 0 && q0 <= q1 && q1 <= ne, 304)) continue;
         for (int q = q0 + lane; q < q1; q += 32) {
           double x[2];
           x[0] = offs[q] * a.scale_d;

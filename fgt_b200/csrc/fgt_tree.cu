@@ -237,7 +237,7 @@ __global__ void k_leaf_ref(const uint32_t* __restrict__ lbox, int nl, const int*
                            const int* __restrict__ parent, int ncutoff, int* __restrict__ lref) {
   for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < nl; o += gridDim.x * blockDim.x) {
     int b = (int)lbox[o];
-    while (level[b] > ncutoff) b = parent[b];
+    while (level[b] > ncutoff && FGT_DCHECK(parent[b] >= 0, 502)) b = parent[b];
     lref[o] = b;
   }
 }
@@ -260,6 +260,7 @@ __global__ void k_point_leaf(const uint64_t* __restrict__ pk, int n,
       int mid = (lo + hi) >> 1;
       if (ls[mid] <= v) lo = mid + 1; else hi = mid;
     }
+    if (!FGT_DCHECK(lo >= 1, 501)) lo = 1;  // every key lies at or after the first leaf
     ord[i] = (uint32_t)(lo - 1);
     idx[i] = (uint32_t)i;
   }

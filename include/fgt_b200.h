@@ -34,6 +34,7 @@ extern "C" {
 #define FGT_ERR_TIMEOUT 5     /* a bounded device wait gave up */
 #define FGT_ERR_NODEVICE 6    /* no CUDA device / library not usable */
 #define FGT_ERR_INJECTED 7    /* host-side fault injection (FGT_FAULT) */
+#define FGT_ERR_CHECK 8       /* a device bounds check failed (FGT_CHECK build only) */
 
 /* precision policy */
 #define FGT_PREC_AUTO 0  /* mixed FP32 bulk when eps >= 1e-6, FP64 otherwise */
@@ -254,6 +255,17 @@ void *fgt_debug_tree_build(int dim, double delta, double eps, int iperiod,
  * (at most cap elements) and returns its length; dst may be NULL. */
 long fgt_debug_tree_get(void *h, const char *name, void *dst, long cap);
 void fgt_debug_tree_free(void *h);
+
+/*
+ * Self-test of the device bounds checks (test support; no counterpart in the
+ * reference, which has no checks).  libfgt_b200_check.so, the FGT_CHECK
+ * build, checks the indexed accesses of its kernels on the device: a failed
+ * check records a site number and skips the access (no trap), and the call
+ * returns FGT_ERR_CHECK naming the first site.  This entry point runs one
+ * kernel on a host-crafted out-of-range index and returns FGT_ERR_CHECK in
+ * that build, FGT_ERR_UNSUPPORTED in the normal one.
+ */
+int fgt_check_selftest(void);
 
 #ifdef __cplusplus
 }
