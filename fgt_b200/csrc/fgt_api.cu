@@ -582,9 +582,14 @@ bool fault_requested(const char* what) {
   return f && strstr(f, what) != nullptr;
 }
 
-// FGT_CHECK build: fail the call when any device bounds check fired during
-// it (the first failing site is named); nothing in the normal build.
+// Device-side failures of a call, read after its last synchronisation:
+// a bounded wait that ran out (FGT_ERR_TIMEOUT) and, in the FGT_CHECK build,
+// a failed bounds check (FGT_ERR_CHECK, the first failing site named).
 void raise_failed_checks(cudaStream_t s) {
+  if (near_wait_status(s) == FGT_ERR_TIMEOUT) {
+    fgt_set_error_message("a bounded wait of the near-field kernel ran out", __FILE__, __LINE__);
+    throw Error{FGT_ERR_TIMEOUT, "a bounded wait of the near-field kernel ran out"};
+  }
 #ifdef FGT_CHECK
   const unsigned site = check_sites(s);
   if (site) {

@@ -3,6 +3,8 @@
 // read as broadcasts.  Mixed precision: FP32 offsets from FP64 box centres,
 // FP32 exp (ex2.approx) and FP32 per-item accumulation, FP64 output
 // accumulation.  FP64 path: same kernel in double.
+#include <stdlib.h>
+
 #include <algorithm>
 
 #include "fgt_direct.cuh"
@@ -632,26 +634,90 @@ __global__ void k_near_lists(NearArgs n) {
   }
 }
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+// ---- bulk asynchronous copies (TMA engine, non-tensor form) with mbarriers
+__device__ __forceinline__ void mbar_init(uint64_t* mb, unsigned count) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(mb);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+// Arrive on the barrier expecting `bytes` of asynchronous writes, then copy
+// `bytes` (a multiple of 16, both addresses 16-byte aligned) global -> shared;
+// the copy's completion counts the bytes off the barrier.
+__device__ __forceinline__ void bulk_load(void* smem, const void* gmem, unsigned bytes,
+                                          uint64_t* mb) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+  const unsigned m = (unsigned)__cvta_generic_to_shared(mb);
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;\n" ::"r"(m),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(d),
+      "l"(gmem), "r"(bytes), "r"(m)
+      : "memory");
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for phase `parity` of the barrier to complete, for at most
+// kWaitLimitNs; false when the limit ran out.
+constexpr uint64_t kWaitLimitNs = 200000000ull;  // 0.2 s
+__device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned parity) {
+  const unsigned m = (unsigned)__cvta_generic_to_shared(mb);
+  uint64_t t0 = 0;
+  for (int it = 0;; it++) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(m), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (it == 0) t0 = global_ns();
+    else if (global_ns() - t0 > kWaitLimitNs) return false;
+  }
+}
+
+// Set on the host thread when the packed kernel was launched, so the status
+// is read back only by calls that ran it.
+thread_local bool t_packed_launched = false;
+
+// Device status of the near-field kernel's waits: FGT_ERR_TIMEOUT when a
+// wait ran out (the kernel then stopped early), read and cleared by the host
+// at the end of a call.
+__device__ int g_near_status;
 
 // k_direct32x2 on packed list-1 sources: a warp item is 64 points of one
 // target box; the box's records are streamed in batches of 32 sources
-// through a double-buffered shared-memory stage filled by asynchronous
-// 16-byte copies (the next batch lands while the current one is summed).
-// Items are taken from a device counter, the next index fetched while the
-// current item runs.  Pair arithmetic as k_direct32x2.
+// (2 KB, contiguous) through a double-buffered shared-memory stage: lane 0
+// issues one bulk copy per batch that completes on the buffer's mbarrier,
+// and the warp waits on it with a time limit (the next batch lands while the
+// current one is summed).  Items are taken from a device counter, the next
+// index fetched while the current item runs.  Pair arithmetic as
+// k_direct32x2.  stall_test != 0 (failure-detection tests only) omits the
+// first copy, so the first wait runs out and the kernel reports
+// FGT_ERR_TIMEOUT.
 template <int DIM, int PGH>
 __global__ void __launch_bounds__(DW * 32) k_direct32x2p(DArgs<float> a, const int* __restrict__ pos,
                                                          const float4* __restrict__ rec,
-                                                         int* __restrict__ next) {
+                                                         int* __restrict__ next, int stall_test) {
   constexpr int NC = 1 + (PGH >= 2 ? DIM : 0);
-  __shared__ __align__(16) float4 stage[DW][2][32 * 4];
+  __shared__ __align__(128) float4 stage[DW][2][32 * 4];
+  __shared__ __align__(8) uint64_t mbar[DW][2];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    mbar_init(&mbar[warp][0], 1);
+    mbar_init(&mbar[warp][1], 1);
+    mbar_init_fence();
+  }
+  __syncwarp();
+  unsigned phase[2] = {0u, 0u};
+  bool first_copy = true;
   const float ce = a.dinv * 1.4426950408889634f;  // exp(-rr/delta) = 2^(-rr*ce)
   const float2 nce = make_float2(-ce, -ce), nrf = make_float2(-a.rfac, -a.rfac);
   const int n_items = *a.n_items_dev;
@@ -667,12 +733,12 @@ __global__ void __launch_bounds__(DW * 32) k_direct32x2p(DArgs<float> a, const i
     const bool actA = pA < ehi, actB = pB < ehi;
     const int c0 = pos[a.l1_ptr[tb]], c1 = pos[a.l1_ptr[tb + 1]];
     // first batch in flight before the target set-up
-    if (c0 + lane < c1) {
-      const float4* g = rec + 4 * (size_t)(c0 + lane);
-#pragma unroll
-      for (int r = 0; r < 4; r++) cp_async16(&stage[warp][0][4 * lane + r], g + r);
+    if (lane == 0 && c0 < c1) {
+      if (!(stall_test && first_copy))
+        bulk_load(stage[warp][0], rec + 4 * (size_t)c0, 64u * (unsigned)min(32, c1 - c0),
+                  &mbar[warp][0]);
+      first_copy = false;
     }
-    cp_async_commit();
     float2 tx[3], txl[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -697,16 +763,21 @@ __global__ void __launch_bounds__(DW * 32) k_direct32x2p(DArgs<float> a, const i
     }
     int buf = 0;
     for (int base = c0; base < c1; base += 32, buf ^= 1) {
-      // issue the next batch into the other buffer, then wait for this one
+      // issue the next batch into the other buffer (read completely by the
+      // warp two batches ago), then wait for this one
       const int nb = base + 32;
-      if (nb + lane < c1) {
-        const float4* g = rec + 4 * (size_t)(nb + lane);
-#pragma unroll
-        for (int r = 0; r < 4; r++) cp_async16(&stage[warp][buf ^ 1][4 * lane + r], g + r);
+      if (lane == 0 && nb < c1)
+        bulk_load(stage[warp][buf ^ 1], rec + 4 * (size_t)nb, 64u * (unsigned)min(32, c1 - nb),
+                  &mbar[warp][buf ^ 1]);
+      const bool ok = mbar_wait(&mbar[warp][buf], phase[buf]);
+      phase[buf] ^= 1u;
+      if (!__all_sync(0xffffffffu, ok)) {
+        // the wait ran out: report, let the other buffer's copy land (also
+        // with a limit) so no copy outlives the block, and stop
+        if (lane == 0) atomicExch(&g_near_status, FGT_ERR_TIMEOUT);
+        if (nb < c1) (void)mbar_wait(&mbar[warp][buf ^ 1], phase[buf ^ 1]);
+        return;
       }
-      cp_async_commit();
-      cp_async_wait1();
-      __syncwarp();
       const float4* S = stage[warp][buf];
       const int cnt = min(32, c1 - base);
 #pragma unroll 4
@@ -855,6 +926,16 @@ long long near_lists_count(const DirectGeom& g, const Lists& L, const int* s_lo,
   return (long long)h;
 }
 
+int near_wait_status(cudaStream_t s) {
+  if (!t_packed_launched) return FGT_OK;
+  t_packed_launched = false;
+  int v = 0, z = 0;
+  FGT_CUDA(cudaMemcpyFromSymbolAsync(&v, g_near_status, sizeof(v), 0, cudaMemcpyDeviceToHost, s));
+  FGT_CUDA(cudaStreamSynchronize(s));
+  if (v) FGT_CUDA(cudaMemcpyToSymbolAsync(g_near_status, &z, sizeof(z), 0, cudaMemcpyHostToDevice, s));
+  return v;
+}
+
 void near_lists_fill(const DirectGeom& g, const Lists& L, const SourceSet<float>& src,
                      const int* t_lo, const int* t_hi, const int* pos, float4* rec,
                      cudaStream_t s) {
@@ -886,10 +967,17 @@ int resident_blocks_p() {
   }
   return nb;
 }
+// FGT_TEST_NEAR_STALL=1 (failure-detection tests only): the packed
+// near-field kernel omits its first copy and must report FGT_ERR_TIMEOUT.
+int near_stall_test() {
+  const char* e = getenv("FGT_TEST_NEAR_STALL");
+  return (e && e[0] == '1') ? 1 : 0;
+}
 template <int DIM, int PGH>
 void launch_packed(const DArgs<float>& a, const NearPacked& p, int* next, cudaStream_t s) {
+  t_packed_launched = true;
   const int grid = std::max(1, std::min(ceil_div(a.n_items, DW), resident_blocks_p<DIM, PGH>()));
-  k_direct32x2p<DIM, PGH><<<grid, DW * 32, 0, s>>>(a, p.pos, p.rec, next);
+  k_direct32x2p<DIM, PGH><<<grid, DW * 32, 0, s>>>(a, p.pos, p.rec, next, near_stall_test());
   FGT_LAUNCH_CHECK();
 }
 }  // namespace

@@ -56,6 +56,11 @@ void near_lists_fill(const DirectGeom& g, const Lists& L, const SourceSet<float>
                      const int* t_lo, const int* t_hi, const int* pos, float4* rec,
                      cudaStream_t s);
 
+// Status of the bounded waits of the packed near-field kernel since the last
+// read: FGT_OK, or FGT_ERR_TIMEOUT when a wait ran out (the kernel stopped
+// early and the results are incomplete).  Clears it; synchronises the stream.
+int near_wait_status(cudaStream_t s);
+
 // Adds the list-1 interactions onto every point of `e`.  Returns the number
 // of kernel launches; *pairs receives the near-field pair count if not null.
 // With packed records (FP32, charges, one density, pgh <= 2) the near field
