@@ -63,6 +63,7 @@ class FgtOpts(C.Structure):
         ("precision", C.c_int), ("device_ptrs", C.c_int), ("device", C.c_int),
         ("stream", C.c_void_p), ("ndiv", C.c_int), ("small_eval", C.c_int),
         ("spread_width", C.c_int), ("timing", C.c_int), ("stats", C.POINTER(FgtStats)),
+        ("root_level", C.c_int),
     ]
 
 
@@ -152,12 +153,15 @@ def _ptr(a):
 
 def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None, rnormal=None,
          ifpgh=1, targets=None, ifpghtarg=0, bs0=1.0, cen0=None, precision=PREC_AUTO,
-         ndiv=0, small_eval=-1, spread_width=0, stats=False, timing=False, check=False):
+         ndiv=0, small_eval=-1, spread_width=0, stats=False, timing=False, check=False,
+         root_level=-1):
     """Point FGT with the reference's argument meaning (src/pfgt/pfgt.f:11-53).
 
     Returns a dict with pot/grad/hess (sources) and pottarg/gradtarg/hesstarg
     (targets) for the requested levels, plus bs0/cen0 (and stats if asked).
     check=True runs the FGT_CHECK build (device bounds checks).
+    root_level >= 0 (free space): bs0/cen0 are inputs and root_level is the
+    cut-off level (a spatial shard of a larger point set).
     """
     L = lib(check)
     src = _f64(sources, (-1, dim))
@@ -189,6 +193,7 @@ def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None, rnorma
     o.spread_width = spread_width
     o.timing = 1 if timing else 0
     o.stats = C.pointer(st) if (stats or timing) else None
+    o.root_level = root_level
     rc = L.fgt_pfgt_c(C.byref(o), nd, dim, delta, eps, iperiod, C.byref(b0),
                       c0.ctypes.data_as(_dp), ns, _ptr(src), ifcharge, _ptr(q), ifdipole,
                       _ptr(rn), _ptr(ds), ifpgh, _ptr(pot), _ptr(grad), _ptr(hess), nt,

@@ -328,10 +328,17 @@ void setup_geometry(Setup& u, const Call& c, double* bs0_io, double* cen0_io, co
   int npwlevel = 0;
   double bs0 = *bs0_io, cen0[FGT_MAXDIM] = {0, 0, 0};
   for (int k = 0; k < dim; k++) cen0[k] = cen0_io[k];
-  tree_setup_scalars(dim, c.delta, c.eps, c.iperiod, c.src, c.ns, c.trg, c.nt, &npwlevel, &bs0,
-                     cen0, s);
-  launches += (c.iperiod != 1) ? 2 : 0;
-  if (c.iperiod != 1) {
+  const bool fixed_root = c.iperiod != 1 && o.root_level >= 0;
+  if (fixed_root) {
+    // a spatial shard: the root box and cut-off level of the whole point set
+    FGT_REQUIRE(bs0 > 0 && isfinite(bs0), FGT_ERR_ARG, "root_level needs bs0 > 0");
+    npwlevel = o.root_level;
+  } else {
+    tree_setup_scalars(dim, c.delta, c.eps, c.iperiod, c.src, c.ns, c.trg, c.nt, &npwlevel, &bs0,
+                       cen0, s);
+    launches += (c.iperiod != 1) ? 2 : 0;
+  }
+  if (c.iperiod != 1 && !fixed_root) {
     *bs0_io = bs0;
     for (int k = 0; k < dim; k++) cen0_io[k] = cen0[k];
   }
@@ -471,18 +478,24 @@ void execute(const Setup& u, const Call& c, const fgt_opts& o, fgt_stats* st, cu
   tm.mark(2);
   // --- plane waves (pfgt.f:700-1073)
   PWWork work;
-  if (u.do_pw && L.n_eval > 0) {
-    PWParams P;
+  PWParams P;
+  PWData<T> D;
+  PWWork* wk = st ? &work : nullptr;
+  const int se = o.small_eval >= 0 ? o.small_eval : -1;
+  const bool pw = u.do_pw && L.n_eval > 0;
+  // Host-buffer calls finish the sources first and copy their outputs to the
+  // host while the targets are evaluated: the two sets are evaluated in two
+  // launches (each box's grid is built twice, which the copy hides).
+  const bool split_sets = c.sources_done && c.ifpgh >= 1 && c.ifpghtarg >= 1 && c.nt > 0;
+  EvalSet<T> none;
+  if (pw) {
     pw_setup(P, dim, nd, u.npw, u.pmax, u.periodic_nodes ? 1 : 0, t.boxsize[0], c.delta, c.eps,
              t.boxsize[t.ncutoff], o.spread_width);
-    PWData<T> D;
-    PWWork* wk = st ? &work : nullptr;
     launches += pw_form<T>(P, t, L, src, D, wk, s);
     tm.mark(4);
     launches += pw_translate<T>(P, L, D, wk, s);
     tm.mark(5);
-    int se = o.small_eval >= 0 ? o.small_eval : -1;
-    launches += pw_eval<T>(P, t, L, D, es, et, se, wk, s);
+    launches += pw_eval<T>(P, t, L, D, es, split_sets ? none : et, se, wk, s);
     tm.mark(6);
     if (st) {
       st->spread_width = P.w;
@@ -514,6 +527,7 @@ void execute(const Setup& u, const Call& c, const fgt_opts& o, fgt_stats* st, cu
       launches++;
     }
     FGT_CUDA(cudaEventRecord(c.sources_done, s));
+    if (pw && split_sets) launches += pw_eval<T>(P, t, L, D, none, et, se, wk, s);
     launches += direct_near_field<T>(g, L, src, et, st ? &pairs : nullptr, s, &packed);
   } else {
     launches += direct_near_field<T>(g, L, src, et, st ? &pairs : nullptr, s, &packed);
@@ -917,6 +931,7 @@ void fgt_opts_default(fgt_opts* o) {
   o->spread_width = 0;
   o->timing = 0;
   o->stats = nullptr;
+  o->root_level = -1;
 }
 
 int fgt_pfgt_c(const fgt_opts* opts, int nd, int dim, double delta, double eps, int iperiod,

@@ -78,6 +78,11 @@ typedef struct fgt_opts {
   int spread_width; /* spreading kernel width in grid cells; 0 = from eps */
   int timing;       /* 1: record per-phase times into stats->ms */
   fgt_stats *stats; /* optional output */
+  int root_level;   /* free space only: >= 0 makes bs0/cen0 inputs and this
+                       the cut-off level (the root box pts_tree_boxsize0,
+                       src/common/pts_tree_nd.f:1330-1414, computed on a
+                       larger point set this call is a spatial shard of);
+                       -1 (default) = computed from the points */
 } fgt_opts;
 
 /* Fill *opts with defaults (precision AUTO, host pointers, current device). */

@@ -108,9 +108,12 @@ def tree(dim, delta, eps, iperiod, sources, targets, bs0=1.0, cen0=None, ndiv=0)
 
 def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None,
          rnormal=None, ifpgh=1, targets=None, ifpghtarg=0, bs0=1.0, cen0=None,
-         quirks=0, nufft="exact"):
+         quirks=0, nufft="exact", root_level=None):
     """Restated reference pfgt; returns dict(pot, grad, hess, pottarg, ...).
 
+    root_level (free space, not None): bs0/cen0 are inputs and the cut-off
+    level is root_level, the geometry of a larger point set this one is a
+    shard of.
     nufft="exact": plane-wave sums by exact non-uniform DFTs (the checker);
     nufft="spread": the restatement's own ES-kernel NUFFT, OpenMP over boxes
     (the timed CPU baseline).  quirks: bit 0/1/2 reproduce the reference's
@@ -135,12 +138,14 @@ def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None,
     ht = np.zeros((max(nt, 1), nhess, nd))
     b0 = C.c_double(float(bs0))
     c0 = np.zeros(3) if cen0 is None else _f64(list(cen0) + [0.0] * (3 - dim))
+    L.oracle_set_root_level(C.c_int(-1 if root_level is None else int(root_level)))
     L.oracle_pfgt(C.c_int(nd), C.c_int(dim), C.c_double(delta), C.c_double(eps),
                   C.c_int(iperiod), C.byref(b0), _p(c0), C.c_int(ns), _p(src),
                   C.c_int(ifcharge), _p(q), C.c_int(ifdipole), _p(rn), _p(ds),
                   C.c_int(ifpgh), _p(pot), _p(grad), _p(hess), C.c_int(nt),
                   _p(trg if nt else np.zeros(1)), C.c_int(ifpghtarg), _p(pt), _p(gt),
                   _p(ht), C.c_int(quirks), C.c_int(1 if nufft == "spread" else 0))
+    L.oracle_set_root_level(C.c_int(-1))
     out = dict(bs0=b0.value, cen0=c0[:dim].copy())
     if ifpgh >= 1:
         out["pot"] = pot[:ns]

@@ -1189,6 +1189,13 @@ void oracle_tree_free(oracle_tree_t *r) {
 
 static int ndiv_for_dim(int dim) { return dim == 1 ? 20 : (dim == 2 ? 80 : 250); }
 
+/* Fixed root box in free space (>= 0): bs0/cen0 are inputs and the cut-off
+ * level is this value, as a shard of a larger point set uses the geometry
+ * pts_tree_boxsize0 computed on the whole set.  -1: the reference's own
+ * computation from the points. */
+static int g_root_level = -1;
+void oracle_set_root_level(int level) { g_root_level = level; }
+
 /* Build the tree and lists exactly as pfgt/pfgtmain do (pfgt.f:110-200,
  * 611-674) and return them.  bs0/cen0 are inputs when iperiod == 1. */
 oracle_tree_t *oracle_tree_build(int dim, double delta, double eps, int iperiod,
@@ -1201,7 +1208,10 @@ oracle_tree_t *oracle_tree_build(int dim, double delta, double eps, int iperiod,
   double bs0 = bs0_in, cen0[MAXDIM] = {0, 0, 0};
   for (k = 0; k < dim; k++) cen0[k] = cen0_in ? cen0_in[k] : 0.0;
   int npwlevel;
-  boxsize0(dim, delta, eps, iperiod, src, ns, trg, nt, &npwlevel, &bs0, cen0);
+  if (g_root_level >= 0 && iperiod != 1)
+    npwlevel = g_root_level;
+  else
+    boxsize0(dim, delta, eps, iperiod, src, ns, trg, nt, &npwlevel, &bs0, cen0);
   int ndiv = ndiv_override > 0 ? ndiv_override : ndiv_for_dim(dim);
   int nlmax = npwlevel >= 0 ? npwlevel + 1 : 0;
   tree_build(&t, dim, src, ns, trg, nt, ndiv, nlmax, iperiod, bs0, cen0);
