@@ -897,6 +897,7 @@ int pw_translate(const PWParams& P, const Lists& L, PWData<T>& D, PWWork* work, 
   std::copy(P.ts.begin(), P.ts.end(), hts);
   FGT_CUDA(cudaMemcpyAsync(ts64.get(), hts, sizeof(double) * P.ts.size(), cudaMemcpyHostToDevice,
                            s));
+  pinned_stage_used(2, s);
   k_wtab<T><<<grid_for((long long)nsh * P.nexp, 256), 256, 0, s>>>(P.dim, P.K, P.nexp, ts64,
                                                                    P.xmin, D.wtab);
   FGT_LAUNCH_CHECK();

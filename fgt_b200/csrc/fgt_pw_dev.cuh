@@ -1121,9 +1121,22 @@ struct DevTables {
 // tables go to the device with one asynchronous copy (a pageable source would
 // make the copy wait for the stream); a slot is rewritten only by a later
 // call, after that call's final stream synchronisation.
+// Event recorded after the last asynchronous copy out of a staging slot; the
+// slot is rewritten only once that copy has run (one call can stage the same
+// slot twice, e.g. the two evaluation launches of a host-buffer call).
+inline cudaEvent_t& pinned_stage_event(int slot) {
+  static thread_local cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  return ev[slot];
+}
+inline void pinned_stage_used(int slot, cudaStream_t s) {
+  cudaEvent_t& e = pinned_stage_event(slot);
+  if (!e) FGT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  FGT_CUDA(cudaEventRecord(e, s));
+}
 inline void* pinned_stage(int slot, size_t bytes) {
   static thread_local void* buf[3] = {nullptr, nullptr, nullptr};
   static thread_local size_t cap[3] = {0, 0, 0};
+  if (cudaEvent_t e = pinned_stage_event(slot)) FGT_CUDA(cudaEventSynchronize(e));
   if (cap[slot] < bytes) {
     if (buf[slot]) cudaFreeHost(buf[slot]);
     buf[slot] = nullptr;
@@ -1211,6 +1224,7 @@ void make_args(const PWParams& P, PWArgs<T>& a, DevTables<T>& tb, cudaStream_t s
   }
   tb.all.alloc(total, s);
   FGT_CUDA(cudaMemcpyAsync(tb.all.get(), h, sizeof(T) * total, cudaMemcpyHostToDevice, s));
+  pinned_stage_used(slot, s);
   T* d = tb.all.get();
   a.twf = d;
   a.twh = d + ntwf;

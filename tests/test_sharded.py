@@ -179,9 +179,11 @@ def test_root_level_option_reproduces_the_free_space_call(fgt):
     a = fgt.pfgt(**kw)
     bs0, cen0, lev = D.root_geometry(3, 3e-3, 1e-6, 0, x.min(axis=0), x.max(axis=0))
     assert bs0 == a["bs0"]
-    b = fgt.pfgt(bs0=bs0, cen0=cen0, root_level=lev, **kw)
-    np.testing.assert_array_equal(a["pot"], b["pot"])
-    np.testing.assert_array_equal(a["grad"], b["grad"])
+    b = fgt.pfgt(bs0=bs0, cen0=cen0, root_level=lev, stats=True, **kw)
+    assert b["stats"]["npwlevel"] == lev and b["stats"]["n_form_boxes"] > 0
+    # same tree; the spreading's shared-memory atomics add in a run-dependent order
+    assert relerr(a["pot"], b["pot"]) < 1e-12
+    assert relerr(a["grad"], b["grad"]) < 1e-12
 
 
 @pytest.mark.gpu
