@@ -48,7 +48,7 @@ class FgtStats(C.Structure):
         ("flops_direct", C.c_double), ("bytes_translate", C.c_double),
         ("pts_form", C.c_double), ("pts_eval_nufft", C.c_double),
         ("pts_eval_modal", C.c_double), ("bs0", C.c_double), ("cen0", C.c_double * 3),
-        ("ms", C.c_double * 12),
+        ("ms", C.c_double * 12), ("small_eval_used", C.c_int), ("tuned", C.c_int),
     ]
 
     def as_dict(self):
@@ -63,7 +63,7 @@ class FgtOpts(C.Structure):
         ("precision", C.c_int), ("device_ptrs", C.c_int), ("device", C.c_int),
         ("stream", C.c_void_p), ("ndiv", C.c_int), ("small_eval", C.c_int),
         ("spread_width", C.c_int), ("timing", C.c_int), ("stats", C.POINTER(FgtStats)),
-        ("root_level", C.c_int),
+        ("root_level", C.c_int), ("autotune", C.c_int),
     ]
 
 
@@ -154,7 +154,7 @@ def _ptr(a):
 def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None, rnormal=None,
          ifpgh=1, targets=None, ifpghtarg=0, bs0=1.0, cen0=None, precision=PREC_AUTO,
          ndiv=0, small_eval=-1, spread_width=0, stats=False, timing=False, check=False,
-         root_level=-1):
+         root_level=-1, autotune=0):
     """Point FGT with the reference's argument meaning (src/pfgt/pfgt.f:11-53).
 
     Returns a dict with pot/grad/hess (sources) and pottarg/gradtarg/hesstarg
@@ -162,6 +162,7 @@ def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None, rnorma
     check=True runs the FGT_CHECK build (device bounds checks).
     root_level >= 0 (free space): bs0/cen0 are inputs and root_level is the
     cut-off level (a spatial shard of a larger point set).
+    autotune: 1 use tuned parameters from the cache, 2 also tune on a miss.
     """
     L = lib(check)
     src = _f64(sources, (-1, dim))
@@ -194,6 +195,7 @@ def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None, rnorma
     o.timing = 1 if timing else 0
     o.stats = C.pointer(st) if (stats or timing) else None
     o.root_level = root_level
+    o.autotune = autotune
     rc = L.fgt_pfgt_c(C.byref(o), nd, dim, delta, eps, iperiod, C.byref(b0),
                       c0.ctypes.data_as(_dp), ns, _ptr(src), ifcharge, _ptr(q), ifdipole,
                       _ptr(rn), _ptr(ds), ifpgh, _ptr(pot), _ptr(grad), _ptr(hess), nt,
@@ -210,7 +212,7 @@ def pfgt(nd, dim, delta, eps, iperiod, sources, charge=None, dipstr=None, rnorma
     return out
 
 
-def pfgt_batch(instances, precision=PREC_AUTO, nworkers=0, ndiv=0, small_eval=-1):
+def pfgt_batch(instances, precision=PREC_AUTO, nworkers=0, ndiv=0, small_eval=-1, autotune=0):
     """Many independent point FGTs in one call (host arrays).
 
     `instances` is a list of dicts with the keyword arguments of `pfgt`
@@ -259,6 +261,7 @@ def pfgt_batch(instances, precision=PREC_AUTO, nworkers=0, ndiv=0, small_eval=-1
     opts.precision = precision
     opts.ndiv = ndiv
     opts.small_eval = small_eval
+    opts.autotune = autotune
     L.fgt_pfgt_batch.restype = C.c_int
     rc = L.fgt_pfgt_batch(C.byref(opts), len(instances), arr, nworkers)
     if rc != FGT_OK:

@@ -580,6 +580,83 @@ void execute(const Setup& u, const Call& c, const fgt_opts& o, fgt_stats* st, cu
   }
 }
 
+// ---------------------------------------------------------------- autotuner
+// Threshold (evaluation points per box) below which a box is evaluated by
+// direct modal sums instead of a grid, when not tuned or given.
+int default_small_eval(int dim) { return dim == 3 ? 48 : (dim == 2 ? 8 : 4); }
+
+// Problem class of a call for the tuning cache: dimension, arithmetic,
+// requested fields, densities, point count (power of two), cut-off level,
+// tree depth and expansion length.
+std::string tune_key(const Setup& u, const Call& c, size_t tsize) {
+  char k[200];
+  long long n = (long long)c.ns + (c.ifpghtarg > 0 ? c.nt : 0);
+  int lg = 0;
+  while ((1ll << (lg + 1)) <= n) lg++;
+  snprintf(k, sizeof(k), "pfgt/v1 dim=%d fp%d pgh=%d,%d nd=%d dip=%d lg2n=%d npwlevel=%d nlevels=%d npw=%d",
+           u.dim, (int)(8 * tsize), c.ifpgh, c.ifpghtarg, c.nd, c.ifdipole ? 1 : 0, lg,
+           u.npwlevel, u.nlevels, u.npw);
+  return k;
+}
+
+// Times the strength-dependent part of the call on its prepared geometry
+// with each candidate modal-evaluation threshold (the workspace rewound
+// after every run, best of two runs each after one warm-up run), stores the
+// fastest under `key` and returns it.  The outputs of these runs are
+// overwritten by the call's final run.
+template <typename T>
+int tune_small_eval(const Setup& u, const Call& c, const fgt_opts& o, cudaStream_t s,
+                    const std::string& key) {
+  static const int c3[] = {0, 16, 32, 48, 64, 96, 128};
+  static const int c2[] = {0, 4, 8, 16, 32, 64};
+  static const int c1[] = {0, 2, 4, 8, 16};
+  const int* cand = u.dim == 3 ? c3 : (u.dim == 2 ? c2 : c1);
+  const int ncand = u.dim == 3 ? 7 : (u.dim == 2 ? 6 : 5);
+  Arena* ar = thread_arena();
+  Timer none(false, s);
+  fgt_opts oo = o;
+  oo.stats = nullptr;
+  oo.timing = 0;
+  cudaEvent_t e0, e1;
+  FGT_CUDA(cudaEventCreate(&e0));
+  FGT_CUDA(cudaEventCreate(&e1));
+  int best = default_small_eval(u.dim);
+  float best_ms = 1e30f;
+  try {
+    auto run = [&](int se) {
+      const std::vector<size_t> m = ar->mark();
+      oo.small_eval = se;
+      execute<T>(u, c, oo, nullptr, s, none);
+      ar->rewind(m);
+    };
+    run(-1);  // module loads and workspace growth
+    for (int i = 0; i < ncand; i++) {
+      float t = 1e30f;
+      for (int rep = 0; rep < 2; rep++) {
+        FGT_CUDA(cudaEventRecord(e0, s));
+        run(cand[i]);
+        FGT_CUDA(cudaEventRecord(e1, s));
+        FGT_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        FGT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        t = std::min(t, ms);
+      }
+      if (t < best_ms) {
+        best_ms = t;
+        best = cand[i];
+      }
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  tune_store(key, best);
+  return best;
+}
+
 template <typename T>
 void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o, fgt_stats* st,
               cudaStream_t s, Timer& tm) {
@@ -588,7 +665,24 @@ void run_pfgt(const Call& c, double* bs0_io, double* cen0_io, const fgt_opts& o,
   const bool near = sizeof(T) == 4 && c.nd == 1 && c.ifcharge && !c.ifdipole && c.ifpgh <= 2 &&
                     c.ifpghtarg <= 2;
   setup_geometry(u, c, bs0_io, cen0_io, o, near, s, tm);
-  execute<T>(u, c, o, st, s, tm);
+  fgt_opts oo = o;
+  int tuned = 0;
+  if (o.autotune > 0 && o.small_eval < 0 && u.do_pw) {
+    const std::string key = tune_key(u, c, sizeof(T));
+    int v = 0;
+    if (tune_lookup(key, v)) {
+      oo.small_eval = v;
+      tuned = 1;
+    } else if (o.autotune >= 2) {
+      oo.small_eval = tune_small_eval<T>(u, c, o, s, key);
+      tuned = 1;
+    }
+  }
+  execute<T>(u, c, oo, st, s, tm);
+  if (st) {
+    st->small_eval_used = oo.small_eval >= 0 ? oo.small_eval : default_small_eval(c.dim);
+    st->tuned = tuned;
+  }
 }
 
 bool fault_requested(const char* what) {
@@ -932,6 +1026,7 @@ void fgt_opts_default(fgt_opts* o) {
   o->timing = 0;
   o->stats = nullptr;
   o->root_level = -1;
+  o->autotune = 0;
 }
 
 int fgt_pfgt_c(const fgt_opts* opts, int nd, int dim, double delta, double eps, int iperiod,

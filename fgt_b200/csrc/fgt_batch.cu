@@ -11,6 +11,7 @@
 // same results.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <functional>
 #include <mutex>
@@ -19,6 +20,7 @@
 
 #include "fgt_b200.h"
 #include "fgt_common.cuh"
+#include "fgt_prims.cuh"
 
 namespace fgt {
 namespace {
@@ -117,6 +119,12 @@ extern "C" int fgt_pfgt_batch(const fgt_opts* opts, int ninst, fgt_instance* ins
   auto weight = [&](int i) { return (long long)inst[i].ns + (inst[i].ifpghtarg > 0 ? inst[i].nt : 0); };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return weight(a) > weight(b); });
   std::atomic<int> next(0);
+  auto run_all = [&](int nwk, const std::function<void(int)>& w) {
+    next = 0;
+    std::lock_guard<std::mutex> lk(g_batch_mutex);
+    if (nwk == 1) w(0);
+    else pool().run(nwk, w);
+  };
   auto work = [&](int) {
     for (;;) {
       const int k = next.fetch_add(1);
@@ -128,11 +136,40 @@ extern "C" int fgt_pfgt_batch(const fgt_opts* opts, int ninst, fgt_instance* ins
                             x.gradtarg, x.hesstarg);
     }
   };
-  {
-    std::lock_guard<std::mutex> lk(g_batch_mutex);
-    if (nw == 1) work(0);
-    else pool().run(nw, work);
+  // autotuner: the worker count of this batch class (instance count and
+  // total points, powers of two), timed over whole batches on the host
+  // clock (the instances run on many streams) after a warm-up batch
+  if (o.autotune > 0 && nworkers <= 0 && ninst > 1) {
+    long long tot = 0;
+    for (int i = 0; i < ninst; i++) tot += weight(i);
+    int lg = 0, lgi = 0;
+    while ((1ll << (lg + 1)) <= tot) lg++;
+    while ((1 << (lgi + 1)) <= ninst) lgi++;
+    char key[96];
+    snprintf(key, sizeof(key), "batch/v1 lg2inst=%d lg2pts=%d", lgi, lg);
+    int v = 0;
+    if (tune_lookup(key, v)) {
+      nw = std::max(1, std::min({v, kMaxWorkers, ninst}));
+    } else if (o.autotune >= 2) {
+      run_all(nw, work);  // warm-up: streams, workspaces, modules
+      double best_t = 1e30;
+      int best = nw;
+      for (int cand : {4, 8, 12, 16, 24}) {
+        const int c = std::max(1, std::min({cand, kMaxWorkers, ninst, hw}));
+        const auto t0 = std::chrono::steady_clock::now();
+        run_all(c, work);
+        cudaDeviceSynchronize();
+        const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (t < best_t) {
+          best_t = t;
+          best = c;
+        }
+      }
+      tune_store(key, best);
+      nw = best;
+    }
   }
+  run_all(nw, work);
   for (int i = 0; i < ninst; i++)
     if (inst[i].status != FGT_OK) return inst[i].status;
   return FGT_OK;

@@ -1,10 +1,77 @@
 // Workspace arena, scans, stable LSD radix sort and searches.
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+
 #include <algorithm>
 #include <map>
+#include <mutex>
 
 #include "fgt_prims.cuh"
 
 namespace fgt {
+
+namespace {
+struct TuneCache {
+  std::mutex mu;
+  bool loaded = false;
+  std::map<std::string, int> kv;
+  std::string path;
+};
+TuneCache& tune_cache() {
+  static TuneCache c;
+  return c;
+}
+std::string tune_path() {
+  const char* e = getenv("FGT_TUNE_CACHE");
+  if (e && *e) return e;
+  const char* h = getenv("HOME");
+  std::string dir = std::string(h && *h ? h : "/tmp") + "/.cache";
+  mkdir(dir.c_str(), 0755);
+  dir += "/fgt_b200";
+  mkdir(dir.c_str(), 0755);
+  return dir + "/tune.txt";
+}
+void tune_load_locked(TuneCache& c) {
+  const std::string p = tune_path();
+  if (c.loaded && p == c.path) return;
+  c.kv.clear();
+  c.path = p;
+  c.loaded = true;
+  FILE* f = fopen(p.c_str(), "r");
+  if (!f) return;
+  char line[512];
+  while (fgets(line, sizeof(line), f)) {
+    char* sp = strrchr(line, ' ');
+    if (!sp) continue;
+    *sp = 0;
+    c.kv[line] = atoi(sp + 1);
+  }
+  fclose(f);
+}
+}  // namespace
+
+bool tune_lookup(const std::string& key, int& value) {
+  TuneCache& c = tune_cache();
+  std::lock_guard<std::mutex> lk(c.mu);
+  tune_load_locked(c);
+  auto it = c.kv.find(key);
+  if (it == c.kv.end()) return false;
+  value = it->second;
+  return true;
+}
+
+void tune_store(const std::string& key, int value) {
+  TuneCache& c = tune_cache();
+  std::lock_guard<std::mutex> lk(c.mu);
+  tune_load_locked(c);
+  c.kv[key] = value;
+  FILE* f = fopen(c.path.c_str(), "a");
+  if (!f) return;  // an unwritable cache only loses the entry
+  fprintf(f, "%s %d\n", key.c_str(), value);
+  fclose(f);
+}
 
 namespace {
 std::vector<CheckReader>& check_readers() {
@@ -59,6 +126,18 @@ void Arena::reset(cudaStream_t s) {
   }
   for (auto& c : chunks) c.off = 0;
   used = 0;
+}
+
+std::vector<size_t> Arena::mark() const {
+  std::vector<size_t> m;
+  for (const auto& c : chunks) m.push_back(c.off);
+  m.push_back(used);
+  return m;
+}
+
+void Arena::rewind(const std::vector<size_t>& m) {
+  for (size_t i = 0; i < chunks.size(); i++) chunks[i].off = i + 1 < m.size() ? m[i] : 0;
+  used = m.empty() ? 0 : m.back();
 }
 
 void Arena::release_all() {

@@ -1,6 +1,7 @@
 // Device primitives: stream-ordered buffers, scans, a stable LSD radix sort,
 // sorted-array searches.  All hand-written; no CUB/Thrust.
 #pragma once
+#include <string>
 #include <vector>
 
 #include "fgt_common.cuh"
@@ -21,6 +22,10 @@ struct Arena {
   void* alloc(size_t bytes);
   void reset(cudaStream_t s);  // call end: all allocations are dead
   void release_all();
+  // Allocation state, and a return to it: buffers allocated after the mark
+  // are dead (their device work is stream-ordered before any later use).
+  std::vector<size_t> mark() const;
+  void rewind(const std::vector<size_t>& m);
 };
 // Arena of the calling host thread on the current device (created lazily),
 // or the arena installed by an ArenaOverride on this thread.
@@ -77,6 +82,13 @@ struct DBuf {
   T* get() const { return p; }
   operator T*() const { return p; }
 };
+
+// On-disk cache of tuned parameters (autotuner): one "key value" line per
+// entry in the file named by FGT_TUNE_CACHE, else
+// $HOME/.cache/fgt_b200/tune.txt; read once per process, appended to on
+// every new entry.  Thread-safe.
+bool tune_lookup(const std::string& key, int& value);
+void tune_store(const std::string& key, int value);
 
 // Exclusive prefix sum of n int32 values (in == out allowed).  If total is not
 // null, the grand total is written to *total (device pointer).

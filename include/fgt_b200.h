@@ -64,6 +64,8 @@ typedef struct fgt_stats {
    * 3 lists, 4 form, 5 translate, 6 eval, 7 direct, 8 scatter, 9 d2h,
    * 10 total */
   double ms[12];
+  int small_eval_used;   /* modal-evaluation threshold the call used */
+  int tuned;             /* 1: parameters came from the tuning cache or a tuning run */
 } fgt_stats;
 
 typedef struct fgt_opts {
@@ -83,6 +85,14 @@ typedef struct fgt_opts {
                        src/common/pts_tree_nd.f:1330-1414, computed on a
                        larger point set this call is a spatial shard of);
                        -1 (default) = computed from the points */
+  int autotune;     /* 0 off (default); 1 take tuned parameters from the
+                       cache; 2 also tune on a cache miss: the call times the
+                       strength-dependent part with each candidate (small_eval
+                       thresholds; worker counts in fgt_pfgt_batch), keeps the
+                       fastest in the cache and returns its results.  Cache:
+                       the file named by FGT_TUNE_CACHE, else
+                       $HOME/.cache/fgt_b200/tune.txt.  Applies only to
+                       parameters left at their defaults. */
 } fgt_opts;
 
 /* Fill *opts with defaults (precision AUTO, host pointers, current device). */
