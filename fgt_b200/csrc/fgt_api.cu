@@ -138,6 +138,88 @@ __global__ void k_gather_out(const double* __restrict__ srt, int n, int nd, int 
   }
 }
 
+// Sorted outputs SoA [comp*nd + id][n] -> AoS [n][comp*nd + id]: one point's
+// components become one contiguous block, so the reorder below reads whole
+// sectors at random positions instead of one 8-byte value per component.
+// Component order (pot, grad_k, hess_m) x density is the order of the
+// reference's per-point blocks of pot(nd,n), grad(nd,dim,n), hess(nd,nh,n).
+// Tiles of 64 points through shared memory: component rows are read
+// coalesced, the tile's AoS block is written contiguously.
+constexpr int AOS_TILE = 64;
+constexpr int AOS_MAXC = 96;  // components per point staged (48 KB per block)
+__global__ void k_to_aos(const double* __restrict__ srt, int n, int ncomp,
+                         double* __restrict__ aos) {
+  __shared__ double tile[AOS_TILE * AOS_MAXC];
+  if (ncomp > AOS_MAXC) {  // many densities: point by point
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+      for (int c = 0; c < ncomp; c++) aos[(size_t)i * ncomp + c] = srt[(size_t)c * n + i];
+    return;
+  }
+  for (int i0 = blockIdx.x * AOS_TILE; i0 < n; i0 += gridDim.x * AOS_TILE) {
+    const int m = min(AOS_TILE, n - i0);
+    for (int idx = threadIdx.x; idx < ncomp * AOS_TILE; idx += blockDim.x) {
+      const int c = idx / AOS_TILE, p = idx - c * AOS_TILE;
+      if (p < m) tile[p * ncomp + c] = srt[(size_t)c * n + i0 + p];
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < m * ncomp; j += blockDim.x) aos[(size_t)i0 * ncomp + j] = tile[j];
+    __syncthreads();
+  }
+}
+
+// out[o] = sorted[inv[o]] for pot/grad/hess in the reference's layouts
+// (dreorderi/dreorderiv, src/common/fmmcommon2d.f:29-90) from the AoS sorted
+// outputs: each point's npot + ngrad + nhess values are contiguous there and
+// in every output array.
+__global__ void k_gather_out_aos(const double* __restrict__ aos, int n, int npot, int ngrad,
+                                 int nhess, const uint32_t* __restrict__ inv,
+                                 double* __restrict__ pot, double* __restrict__ grad,
+                                 double* __restrict__ hess) {
+  const int nc = npot + ngrad + nhess;
+  const int st = gridDim.x * blockDim.x;
+  for (int o0 = blockIdx.x * blockDim.x + threadIdx.x; o0 < n; o0 += UB * st) {
+    size_t iu[UB];
+#pragma unroll
+    for (int u = 0; u < UB; u++) {
+      iu[u] = o0 + u * st < n ? inv[o0 + u * st] : 0;
+      if (!FGT_DCHECK(iu[u] < (size_t)n, 106)) iu[u] = 0;
+    }
+#pragma unroll
+    for (int u = 0; u < UB; u++) {
+      const size_t o = (size_t)o0 + (size_t)u * st;
+      if (o >= (size_t)n) break;
+      const double* a = aos + iu[u] * nc;
+      for (int c = 0; c < npot; c++) pot[o * npot + c] = a[c];
+      for (int c = 0; c < ngrad; c++) grad[o * ngrad + c] = a[npot + c];
+      for (int c = 0; c < nhess; c++) hess[o * nhess + c] = a[npot + ngrad + c];
+    }
+  }
+}
+
+// Reorder of one evaluation set's sorted outputs to the caller's layout.
+// Up to 7 components per point the gather reads them straight from the SoA
+// arrays (a few sectors per point); from 8 on (several densities, hessians)
+// the outputs are first transposed to AoS so a point's components are one
+// contiguous read (config-3-like calls: nd = 4, pot + grad).
+void reorder_outputs(const double* srt, int n, int nd, int dim, int pgh, const uint32_t* inv,
+                     double* pot, double* grad, double* hess, cudaStream_t s, int& launches) {
+  const int nh = dim * (dim + 1) / 2;
+  const int npot = nd, ngrad = pgh >= 2 ? nd * dim : 0, nhess = pgh >= 3 ? nd * nh : 0;
+  if (npot + ngrad + nhess < 8) {
+    k_gather_out<<<grid_for(n, 256), 256, 0, s>>>(srt, n, nd, dim, pgh, inv, pot, grad, hess);
+    FGT_LAUNCH_CHECK();
+    launches++;
+    return;
+  }
+  DBuf<double> aos((size_t)n * (npot + ngrad + nhess), s);
+  k_to_aos<<<grid_for(n, AOS_TILE * 4, 8), 256, 0, s>>>(srt, n, npot + ngrad + nhess, aos);
+  FGT_LAUNCH_CHECK();
+  k_gather_out_aos<<<grid_for(n, 256), 256, 0, s>>>(aos, n, npot, ngrad, nhess, inv, pot, grad,
+                                                     hess);
+  FGT_LAUNCH_CHECK();
+  launches += 2;
+}
+
 struct DevicePool {
   bool configured = false;
 };
@@ -520,12 +602,8 @@ void execute(const Setup& u, const Call& c, const fgt_opts& o, fgt_stats* st, cu
   if (c.sources_done) {
     // sources first, then signal; the targets follow
     launches += direct_near_field<T>(g, L, src, es, st ? &pairs : nullptr, s, &packed);
-    if (c.ifpgh >= 1) {
-      k_gather_out<<<grid_for(c.ns, 256), 256, 0, s>>>(outs, c.ns, nd, dim, c.ifpgh, u.inv_s,
-                                                       c.pot, c.grad, c.hess);
-      FGT_LAUNCH_CHECK();
-      launches++;
-    }
+    if (c.ifpgh >= 1)
+      reorder_outputs(outs, c.ns, nd, dim, c.ifpgh, u.inv_s, c.pot, c.grad, c.hess, s, launches);
     FGT_CUDA(cudaEventRecord(c.sources_done, s));
     if (pw && split_sets) launches += pw_eval<T>(P, t, L, D, none, et, se, wk, s);
     launches += direct_near_field<T>(g, L, src, et, st ? &pairs : nullptr, s, &packed);
@@ -535,18 +613,11 @@ void execute(const Setup& u, const Call& c, const fgt_opts& o, fgt_stats* st, cu
   }
   tm.mark(7);
   // --- back to input order
-  if (c.ifpgh >= 1 && !c.sources_done) {
-    k_gather_out<<<grid_for(c.ns, 256), 256, 0, s>>>(outs, c.ns, nd, dim, c.ifpgh, u.inv_s, c.pot,
-                                                     c.grad, c.hess);
-    FGT_LAUNCH_CHECK();
-    launches++;
-  }
-  if (c.ifpghtarg >= 1 && c.nt > 0) {
-    k_gather_out<<<grid_for(c.nt, 256), 256, 0, s>>>(outt, c.nt, nd, dim, c.ifpghtarg, u.inv_t,
-                                                     c.pott, c.gradt, c.hesst);
-    FGT_LAUNCH_CHECK();
-    launches++;
-  }
+  if (c.ifpgh >= 1 && !c.sources_done)
+    reorder_outputs(outs, c.ns, nd, dim, c.ifpgh, u.inv_s, c.pot, c.grad, c.hess, s, launches);
+  if (c.ifpghtarg >= 1 && c.nt > 0)
+    reorder_outputs(outt, c.nt, nd, dim, c.ifpghtarg, u.inv_t, c.pott, c.gradt, c.hesst, s,
+                    launches);
   tm.mark(8);
   if (st) {
     st->nlevels = u.nlevels;
