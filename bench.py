@@ -45,6 +45,9 @@ def parse():
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--profile-once", action="store_true",
                    help="one untimed step only (for ncu launch lists)")
+    p.add_argument("--profile-config", type=int, default=5, choices=[1, 2, 3, 5],
+                   help="configuration of the --profile-once step (--scale, and --delta/--eps "
+                        "for configuration 3 and 5, apply)")
     p.add_argument("--sweep", default="cells", choices=["none", "cells", "all"],
                    help="also time the benchmark's other configurations: 'cells' = the "
                         "delta/eps cells of the sphere workload at eps=1e-6 plus configs 1-3, "
@@ -525,7 +528,13 @@ def main():
                       pt_d.data_ptr(), gt_d.data_ptr(), None)
 
     if a.profile_once:
-        step_dev()
+        if a.profile_config == 5:
+            step_dev()
+        else:
+            pc = W.config(a.profile_config, scale=a.scale)
+            if a.profile_config == 3:
+                pc["delta"], pc["eps"] = a.delta, a.eps
+            run_cell(F, dev, stream, pc, prec, 1, 0)
         torch.cuda.synchronize()
         return
 
@@ -790,6 +799,9 @@ def main():
         torch.cuda.empty_cache()
         cells = sweep(a, F, dev, stream, W)
     roof = roofline(a, stats, ms_phase)
+    rho = ncu_traffic().get("translate_l2_read_miss_fraction")
+    if rho is not None:
+        roof["translate_rho"] = rho  # fraction of translation reads that miss L2 (ncu)
     if roof.get("traffic") is not None:
         roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
                                   "of the kernel on the 0.3-scale workload, scaled to this size "

@@ -654,7 +654,10 @@ void launch_form_small2(PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp,
   const int nw = small2_warps<T>(a.g, smem);
   auto k = k_form_small2<T, W>;
   set_smem(k, smem);
-  k<<<kSMs * std::max(1, 8 / nw), 32 * nw, smem, s>>>(a, io, fp, order, first, next);
+  // as many 8-warp CTAs per SM as the shared memory allows (the warps of a
+  // CTA share only the staged tables; more CTAs hide more latency)
+  const int per_sm = std::max(1, std::min(8, (int)((size_t)(228 * 1024) / (smem + 1024))));
+  k<<<kSMs * per_sm, 32 * nw, smem, s>>>(a, io, fp, order, first, next);
   FGT_LAUNCH_CHECK();
 }
 template <typename T>

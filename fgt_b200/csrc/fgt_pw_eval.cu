@@ -734,7 +734,10 @@ void launch_eval_small2(PWArgs<T>& a, const EvalPtrs<T>& ep, const int* first, i
   const int nw = small2_eval_warps<T>(a.g, smem);
   auto k = k_eval_small2<T, W, DERIV>;
   set_smem(k, smem);
-  k<<<kSMs * std::max(1, 8 / nw), 32 * nw, smem, s>>>(a, ep, first, next);
+  // as many 8-warp CTAs per SM as the shared memory allows (the warps of a
+  // CTA share only the staged tables; more CTAs hide more latency)
+  const int per_sm = std::max(1, std::min(8, (int)((size_t)(228 * 1024) / (smem + 1024))));
+  k<<<kSMs * per_sm, 32 * nw, smem, s>>>(a, ep, first, next);
   FGT_LAUNCH_CHECK();
 }
 template <typename T>
