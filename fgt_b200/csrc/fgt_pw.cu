@@ -41,16 +41,23 @@ struct FormPtrs {
 // shared-memory atomic per non-zero cell, instead of W^3 atomics per point.
 constexpr int TB = 4;           // block edge (base cells)
 constexpr int NBLK_MAX = 1024;  // blocks per box
-constexpr int FCH = 8192;       // points sorted per round
 constexpr int PB = 8;           // points per warp batch
 constexpr int TP = 12;          // padded kernel row (TILE <= TP - 1)
+// points sorted per round: FP32 8192; FP64 2048 (its ~200 KB grid leaves
+// little shared memory)
+template <typename T>
+__host__ __device__ constexpr int fch() {
+  return sizeof(T) == 4 ? 8192 : 2048;
+}
 
 // byte offset of the grid buffer in the tiled form kernel; every part is a
-// multiple of 16 bytes, so the kernel-row buffer is float4 aligned
+// multiple of 16 bytes, so the kernel-row buffer is float4 aligned.  The
+// FP64 variant takes its kernel rows from warp shuffles (no row buffer).
 template <typename T>
 __host__ __device__ constexpr size_t tiled_offset(int G, int K) {
-  return tw_bytes16<T>(G, K) + sizeof(int) * (2 * NBLK_MAX + 32) + sizeof(int) * FCH +
-         sizeof(unsigned short) * FCH + sizeof(float) * (PW_THREADS / 32) * PB * 3 * TP;
+  return tw_bytes16<T>(G, K) + sizeof(int) * (2 * NBLK_MAX + 32) + sizeof(int) * fch<T>() +
+         sizeof(unsigned short) * fch<T>() +
+         (sizeof(T) == 4 ? sizeof(float) * (PW_THREADS / 32) * PB * 3 * TP : 0);
 }
 
 // Exclusive scan of cnt[0..n) into off[0..n) for n <= 2 * blockDim.x;
@@ -208,6 +215,115 @@ __device__ void spread_tiled(const PWArgs<T>& a, T* B, const double* __restrict_
   __syncthreads();
 }
 
+// FP64 block-tiled spreading (3D, eps >= ~1e-6): as spread_tiled, with
+// blocks of TBD^3 base cells, a register tile of (TBD+W-1)^3 FP64 cells
+// (lane l owns the tile columns l, l+32, ... with all TILE z cells), and the
+// point's three kernel rows taken from warp shuffles: lanes 0..3W-1 each
+// evaluate one kernel value (dimension lane/W, offset lane%W) per point.  The
+// flush adds every non-zero tile cell with one atomic: ~TILE^3/(points per
+// block) atomics per point instead of W^3.
+template <int W, int TBD>
+__device__ void spread_tiled_d(const PWArgs<double>& a, double* B, const double* __restrict__ off,
+                               int ns, const double* __restrict__ sq,
+                               const double* __restrict__ sr, bool is_q, int c0, int n, int* cnt,
+                               int* boff, int* misc, int* tmp, unsigned short* perm) {
+  constexpr int TILE = TBD + W - 1, NCOL = (TILE * TILE + 31) / 32;
+  static_assert(3 * W <= 32, "one kernel value per lane");
+  const Geo& g = a.g;
+  const int nbd = (g.G - W + 1 + TBD - 1) / TBD, nblk = nbd * nbd * nbd;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) cnt[i] = 0;
+  if (threadIdx.x == 0) misc[0] = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int blk = 0;
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      blk = blk * nbd + base_cell<double, W>(a, off[(size_t)d * ns + c0 + i] * a.scale_d) / TBD;
+    const int r = atomicAdd(&cnt[blk], 1);
+    tmp[i] = (r << 10) | blk;
+  }
+  __syncthreads();
+  block_scan(cnt, boff, nblk, misc + 1);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int v = tmp[i];
+    perm[boff[v & (NBLK_MAX - 1)] + (v >> 10)] = (unsigned short)i;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  int cx[NCOL], cy[NCOL];
+#pragma unroll
+  for (int j = 0; j < NCOL; j++) {
+    const int c = lane + 32 * j;
+    cx[j] = c < TILE * TILE ? c / TILE : -1;
+    cy[j] = c < TILE * TILE ? c % TILE : -1;
+  }
+  const int kd = lane / W, kj = lane - kd * W;  // this lane's kernel value
+  for (;;) {
+    int bi = 0;
+    if (lane == 0) bi = atomicAdd(&misc[0], 1);
+    bi = __shfl_sync(0xffffffffu, bi, 0);
+    if (bi >= nblk) break;
+    const int nb = cnt[bi];
+    if (nb == 0) continue;
+    const int start = boff[bi];
+    int org[3];
+    org[2] = (bi % nbd) * TBD;
+    org[1] = ((bi / nbd) % nbd) * TBD;
+    org[0] = (bi / (nbd * nbd)) * TBD;
+    double acc[NCOL][TILE];
+#pragma unroll
+    for (int j = 0; j < NCOL; j++)
+#pragma unroll
+      for (int t = 0; t < TILE; t++) acc[j][t] = 0.0;
+    for (int k = 0; k < nb; k++) {
+      const int pt = c0 + perm[start + k];
+      // stencil offsets in the tile (all lanes) and this lane's kernel value
+      int o[3];
+      double v = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const double x = off[(size_t)d * ns + pt] * a.scale_d;
+        double f0;
+        const int i0 = kernel_start<double>(a, x, f0);
+        int b = i0 - g.l0;
+        b = b < 0 ? 0 : (b > g.G - W ? g.G - W : b);
+        o[d] = b - org[d];
+        if (d == kd && lane < 3 * W) v = es_kernel<double>((f0 + (double)kj) * a.inv_hw, a.beta);
+      }
+      const double sc = is_q ? sq[pt] : sq[pt] * sr[pt];
+      double pz[TILE];
+#pragma unroll
+      for (int t = 0; t < TILE; t++) {
+        const int jz = t - o[2];
+        const double z = __shfl_sync(0xffffffffu, v, 2 * W + (jz < 0 ? 0 : (jz >= W ? W - 1 : jz)));
+        pz[t] = (jz >= 0 && jz < W) ? z : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < NCOL; j++) {
+        const int jx = cx[j] - o[0], jy = cy[j] - o[1];
+        const double px = __shfl_sync(0xffffffffu, v, jx < 0 ? 0 : (jx >= W ? W - 1 : jx));
+        const double py = __shfl_sync(0xffffffffu, v, W + (jy < 0 ? 0 : (jy >= W ? W - 1 : jy)));
+        const bool in = jx >= 0 && jx < W && jy >= 0 && jy < W;
+        const double pxy = in ? px * py * sc : 0.0;
+#pragma unroll
+        for (int t = 0; t < TILE; t++) acc[j][t] = fma(pxy, pz[t], acc[j][t]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < NCOL; j++) {
+      const int x = org[0] + cx[j], y = org[1] + cy[j];
+      if (cx[j] >= 0 && x < g.G && y < g.G) {
+        double* col = B + x * g.str[0] + y * g.str[1] + org[2];
+#pragma unroll
+        for (int t = 0; t < TILE; t++)
+          if (org[2] + t < g.G && acc[j][t] != 0.0) atomicAdd(col + t, acc[j][t]);
+      }
+    }
+  }
+  __syncthreads();
+}
+constexpr int TB_D = 2;  // FP64 block edge (register tile of 3 x 9 columns, no spills)
+
 template <typename T, int DIM, int W, bool GB, bool TILED>
 __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, FormPtrs<T> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -215,24 +331,23 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
   const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
   T* sm = reinterpret_cast<T*>(smem_raw);
   const int NFp = pad4(NF), NHp = pad4(NH);
-  T* twf = sm;                 // G*NF complex, planar rows of 2*NFp
-  T* twh = twf + 2 * G * NFp;  // G*NH complex, planar rows of 2*NHp
+  // G*NF and G*NH complex, planar rows of 2*NFp / 2*NHp (staged or global)
+  const T* twf = stage_tw(sm, a.twf, 2 * G * NFp);
+  const T* twh = stage_tw(sm + 2 * G * NFp, a.twh, 2 * G * NHp);
   // atomic-spreading scratch
-  int* ordtmp = reinterpret_cast<int*>(sm + tw_elems(G, K));  // ORDER_CHUNK
+  int* ordtmp = reinterpret_cast<int*>(sm + tw_elems_t<T>(G, K));  // ORDER_CHUNK
   int* ordcnt = ordtmp + ORDER_CHUNK;                        // 32
   unsigned short* perm = reinterpret_cast<unsigned short*>(ordcnt + 32);  // ORDER_CHUNK
   // tiled-spreading scratch
   int* tcnt = reinterpret_cast<int*>(smem_raw + tw_bytes16<T>(G, K));  // NBLK_MAX
   int* toff = tcnt + NBLK_MAX;                             // NBLK_MAX
   int* tmisc = toff + NBLK_MAX;                            // 32
-  int* ttmp = tmisc + 32;                                  // FCH
-  unsigned short* tperm = reinterpret_cast<unsigned short*>(ttmp + FCH);  // FCH
-  T* trows = reinterpret_cast<T*>(tperm + FCH);  // warps * PB * 3 * TP
+  int* ttmp = tmisc + 32;                                  // fch
+  unsigned short* tperm = reinterpret_cast<unsigned short*>(ttmp + fch<T>());  // fch
+  T* trows = reinterpret_cast<T*>(tperm + fch<T>());  // FP32: warps * PB * 3 * TP
   T* B = GB ? a.gscratch + (size_t)blockIdx.x * g.bufsz
             : reinterpret_cast<T*>(smem_raw + (TILED ? tiled_offset<T>(G, K)
                                                      : order_offset<T>(G, K)));
-  load_tw(twf, a.twf, 2 * G * NFp);
-  load_tw(twh, a.twh, 2 * G * NHp);
   __syncthreads();
   // items in decreasing source count, each CTA takes the next one; the
   // parts of a split box write partial expansions, summed by k_form_reduce
@@ -264,9 +379,14 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
         if constexpr (TILED) {
           const T* sq = is_q ? p.q + (size_t)id * io.ns : p.ds + (size_t)id * io.ns;
           const T* sr = is_q ? nullptr : p.rn + (size_t)dd * io.ns;
-          for (int c0 = p0; c0 < p1; c0 += FCH)
-            spread_tiled<T, W>(a, B, p.off, io.ns, sq, sr, is_q, c0, min(FCH, p1 - c0), tcnt, toff,
-                               tmisc, ttmp, tperm, trows);
+          for (int c0 = p0; c0 < p1; c0 += fch<T>()) {
+            if constexpr (std::is_same<T, double>::value)
+              spread_tiled_d<W, TB_D>(a, B, p.off, io.ns, sq, sr, is_q, c0, min(fch<T>(), p1 - c0),
+                                      tcnt, toff, tmisc, ttmp, tperm);
+            else
+              spread_tiled<T, W>(a, B, p.off, io.ns, sq, sr, is_q, c0, min(fch<T>(), p1 - c0),
+                                 tcnt, toff, tmisc, ttmp, tperm, trows);
+          }
         } else {
           for (int c0 = p0; c0 < p1; c0 += ORDER_CHUNK) {
             const int n = min(ORDER_CHUNK, p1 - c0);
@@ -361,10 +481,9 @@ __global__ void __launch_bounds__(256) k_form_small2(PWArgs<T> a, FormIO io, For
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geo& g = a.g;
   const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
-  T* twf = reinterpret_cast<T*>(smem_raw);
-  T* twh = twf + 2 * G * pad4(NF);
-  load_tw(twf, a.twf, 2 * G * pad4(NF));
-  load_tw(twh, a.twh, 2 * G * pad4(NH));
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const T* twf = stage_tw(sm, a.twf, 2 * G * pad4(NF));
+  const T* twh = stage_tw(sm + 2 * G * pad4(NF), a.twh, 2 * G * pad4(NH));
   const Small2Layout lay = small2_layout(G, K);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* A = reinterpret_cast<T*>(smem_raw + tw_bytes16<T>(G, K)) + (size_t)warp * lay.per_warp;
@@ -598,6 +717,17 @@ int launch_form(PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>& 
   int grid = std::max(1, std::min(io.max_items, kSMs));
   if constexpr (std::is_same<T, float>::value && DIM == 3 && TB + W - 1 <= TP - 1) {
     const int nbd = (a.g.G - W + 1 + TB - 1) / TB;
+    const size_t tneed = tiled_offset<T>(a.g.G, a.g.K) + sizeof(T) * (size_t)a.g.bufsz;
+    if (!a.g.wrap && nbd * nbd * nbd <= NBLK_MAX && tneed <= (size_t)MAXSMEM) {
+      auto k = k_form<T, DIM, W, false, true>;
+      set_smem(k, tneed);
+      k<<<grid, PW_THREADS, tneed, s>>>(a, io, fp);
+      FGT_LAUNCH_CHECK();
+      return 1;
+    }
+  }
+  if constexpr (std::is_same<T, double>::value && DIM == 3 && W <= 8) {
+    const int nbd = (a.g.G - W + 1 + TB_D - 1) / TB_D;
     const size_t tneed = tiled_offset<T>(a.g.G, a.g.K) + sizeof(T) * (size_t)a.g.bufsz;
     if (!a.g.wrap && nbd * nbd * nbd <= NBLK_MAX && tneed <= (size_t)MAXSMEM) {
       auto k = k_form<T, DIM, W, false, true>;

@@ -68,17 +68,28 @@ __host__ __device__ constexpr size_t tw_elems(int G, int K) {
                           : (size_t)pad4(G) * (3 * K + 2));
 }
 
-// twiddle tables, rounded up to 16 bytes (scratch or grids follow)
+// Where the kernels read the twiddle tables: staged in shared memory (FP32),
+// or from global memory through the L1 cache (FP64: the 8-byte grids of the
+// eps = 1e-6 cells, ~200 KB, only fit in shared memory without the tables).
+template <typename T>
+__host__ __device__ constexpr bool tw_in_smem() {
+  return sizeof(T) == 4;
+}
+template <typename T>
+__host__ __device__ constexpr size_t tw_elems_t(int G, int K) {
+  return tw_in_smem<T>() ? tw_elems(G, K) : 0;
+}
+// twiddle tables in shared memory, rounded up to 16 bytes (scratch or grids follow)
 template <typename T>
 __host__ __device__ constexpr size_t tw_bytes16(int G, int K) {
-  return ((size_t)sizeof(T) * tw_elems(G, K) + 15) & ~(size_t)15;
+  return ((size_t)sizeof(T) * tw_elems_t<T>(G, K) + 15) & ~(size_t)15;
 }
 
 // byte offset of the grid buffer in shared memory: twiddles, then the
 // ordering scratch (ORDER_CHUNK ints + 32 counters + ORDER_CHUNK u16)
 template <typename T>
 __host__ __device__ constexpr size_t order_offset(int G, int K) {
-  return (((size_t)sizeof(T) * tw_elems(G, K) + sizeof(int) * (ORDER_CHUNK + 32) +
+  return (((size_t)sizeof(T) * tw_elems_t<T>(G, K) + sizeof(int) * (ORDER_CHUNK + 32) +
            sizeof(unsigned short) * ORDER_CHUNK) + 15) &
          ~(size_t)15;
 }
@@ -833,7 +844,8 @@ __device__ __forceinline__ void order_cells(const PWArgs<T>& a, const double* of
 // scratch of order_offset, then the cell-order bins and scan workspace
 template <typename T>
 __host__ __device__ constexpr size_t eval_offset(int G, int K) {
-  return order_offset<T>(G, K) + sizeof(int) * (NBINS_MAX + 32);
+  // FP32: the cell-order bins; FP64 grids use the bank-class order (no bins)
+  return order_offset<T>(G, K) + (sizeof(T) == 4 ? sizeof(int) * (NBINS_MAX + 32) : 0);
 }
 
 // Keys of a longest-processing-time order: entry i of a box list (list[i]
@@ -1102,6 +1114,16 @@ __device__ __forceinline__ void warp_pass_c2c(const T* C, int SC, int nin, int n
 template <typename T>
 __device__ __forceinline__ void load_tw(T* dst, const T* src, int n) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+// A twiddle table for the kernel: staged at `smem` (FP32) or read in place.
+template <typename T>
+__device__ __forceinline__ const T* stage_tw(T* smem, const T* src, int n) {
+  if constexpr (tw_in_smem<T>()) {
+    load_tw(smem, src, n);
+    return smem;
+  } else {
+    return src;
+  }
 }
 
 int supported_w(int w) {

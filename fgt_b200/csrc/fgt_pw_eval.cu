@@ -141,9 +141,10 @@ __global__ void __launch_bounds__(eval_threads<T, DIM, W, GB, DERIV>())
   const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
   T* sm = reinterpret_cast<T*>(smem_raw);
   const int Gp = pad4(G);
-  T* tif = sm;                 // planar rows of 2*Gp
-  T* tih = tif + 2 * NF * Gp;
-  int* ordtmp = reinterpret_cast<int*>(sm + tw_elems(G, K));
+  // planar rows of 2*Gp (staged or global)
+  const T* tif = stage_tw(sm, a.tif, 2 * NF * Gp);
+  const T* tih = stage_tw(sm + 2 * NF * Gp, a.tih, 2 * NH * Gp);
+  int* ordtmp = reinterpret_cast<int*>(sm + tw_elems_t<T>(G, K));
   int* ordcnt = ordtmp + ORDER_CHUNK;
   unsigned short* perm = reinterpret_cast<unsigned short*>(ordcnt + 32);
   int* bins = reinterpret_cast<int*>(smem_raw + order_offset<T>(G, K));  // NBINS_MAX
@@ -155,8 +156,6 @@ __global__ void __launch_bounds__(eval_threads<T, DIM, W, GB, DERIV>())
     if constexpr (GB) return static_cast<const T*>(B);
     else return SmemView<T>{(int)(eval_offset<T>(G, K) / sizeof(T))};
   }();
-  load_tw(tif, a.tif, 2 * NF * Gp);
-  load_tw(tih, a.tih, 2 * NH * Gp);
   __syncthreads();
   // shared-space byte address of the grid (shared-memory grid variants)
   const uint32_t grid_saddr =
@@ -567,10 +566,9 @@ __global__ void __launch_bounds__(256) k_eval_small2(PWArgs<T> a, EvalPtrs<T> p,
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geo& g = a.g;
   const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G, Gp = pad4(G);
-  T* tif = reinterpret_cast<T*>(smem_raw);
-  T* tih = tif + 2 * NF * Gp;
-  load_tw(tif, a.tif, 2 * NF * Gp);
-  load_tw(tih, a.tih, 2 * NH * Gp);
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const T* tif = stage_tw(sm, a.tif, 2 * NF * Gp);
+  const T* tih = stage_tw(sm + 2 * NF * Gp, a.tih, 2 * NH * Gp);
   const Small2Layout lay = small2_layout(G, K);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* R1 = reinterpret_cast<T*>(smem_raw + tw_bytes16<T>(G, K)) + (size_t)warp * lay.per_warp;
@@ -697,7 +695,8 @@ int launch_eval_k(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t
     // order_cells spreads the bins over whole rounds of the CTA's threads
     const long nthr = eval_threads<T, DIM, W, false, DERIV>();
     const long padded = (nbins + nthr - 1) / nthr * nthr;
-    epk.cell_bins = (!a.g.wrap && nb > 0 && padded <= NBINS_MAX) ? (int)nbins : 0;
+    epk.cell_bins =
+        (sizeof(T) == 4 && !a.g.wrap && nb > 0 && padded <= NBINS_MAX) ? (int)nbins : 0;
   }
   if (gb) {
     gs.alloc((size_t)grid * a.g.bufsz, s);
