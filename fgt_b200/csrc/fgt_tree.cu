@@ -266,6 +266,26 @@ __global__ void k_point_leaf(const uint64_t* __restrict__ pk, int n,
   }
 }
 
+// Dense leaf table of the finest cells (small key spaces): the leaves'
+// start keys, sorted, cut the 2^(dim*D) cells into the leaves' ranges;
+// table[c] = ordinal of the leaf whose range holds cell c.
+__global__ void k_cell_leaf(const uint64_t* __restrict__ ls, int nl, long long ncell,
+                            uint32_t* __restrict__ table) {
+  for (int o = blockIdx.x; o < nl; o += gridDim.x) {
+    const long long c0 = (long long)ls[o], c1 = o + 1 < nl ? (long long)ls[o + 1] : ncell;
+    for (long long c = c0 + threadIdx.x; c < c1; c += blockDim.x) table[c] = (uint32_t)o;
+  }
+}
+// Leaf ordinal of each point by the dense table (value: the original index).
+__global__ void k_point_leaf_dense(const uint64_t* __restrict__ pk, int n,
+                                   const uint32_t* __restrict__ table, uint32_t* __restrict__ ord,
+                                   uint32_t* __restrict__ idx) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    ord[i] = table[pk[i]];
+    idx[i] = (uint32_t)i;
+  }
+}
+
 // leaf_lo[o] = first sorted position with ordinal >= o, o = 0..nl
 __global__ void k_leaf_point_lo(const uint32_t* __restrict__ ord, int n, int nl,
                                 int* __restrict__ lo) {
@@ -525,9 +545,22 @@ void tree_build(Tree& t, int dim, int iperiod, int npwlevel, int ndiv, double bs
     DBuf<uint32_t> vtmp(std::max(std::max(ns, nt), 1), s);
     uint32_t* otmp = reinterpret_cast<uint32_t*>(ktmp.get());  // >= max(ns, nt) u32
     t.isrc.alloc(std::max(ns, 1), s);
-    if (ns > 0) {
-      k_point_leaf<<<grid_for(ns, 256), 256, 0, s>>>(skey, ns, ls, nl, ord, t.isrc);
+    DBuf<uint32_t> table;
+    if (dense && nl > 0) {  // leaf ordinals by table lookup instead of binary search
+      const long long ncell = 1ll << (dim * D);
+      table.alloc((size_t)ncell, s);
+      k_cell_leaf<<<std::min(nl, kSMs * 16), 256, 0, s>>>(ls, nl, ncell, table);
       FGT_LAUNCH_CHECK();
+    }
+    auto point_leaf = [&](const uint64_t* keys, int n, uint32_t* o, uint32_t* idx) {
+      if (table.p)
+        k_point_leaf_dense<<<grid_for(n, 256), 256, 0, s>>>(keys, n, table, o, idx);
+      else
+        k_point_leaf<<<grid_for(n, 256), 256, 0, s>>>(keys, n, ls, nl, o, idx);
+      FGT_LAUNCH_CHECK();
+    };
+    if (ns > 0) {
+      point_leaf(skey, ns, ord, t.isrc);
       radix_sort_u32(ord, t.isrc, otmp, vtmp, ns, obits, s);
     }
     k_leaf_point_lo<<<grid_for(nl + 1, 256), 256, 0, s>>>(ord, ns, nl, slo);
@@ -539,8 +572,7 @@ void tree_build(Tree& t, int dim, int iperiod, int npwlevel, int ndiv, double bs
     DBuf<uint32_t> tord(std::max(nt, 1), s);
     t.itrg.alloc(std::max(nt, 1), s);
     if (nt > 0) {
-      k_point_leaf<<<grid_for(nt, 256), 256, 0, s>>>(tkey, nt, ls, nl, tord, t.itrg);
-      FGT_LAUNCH_CHECK();
+      point_leaf(tkey, nt, tord, t.itrg);
       radix_sort_u32(tord, t.itrg, otmp, vtmp, nt, obits, s);
     }
     k_leaf_point_lo<<<grid_for(nl + 1, 256), 256, 0, s>>>(tord, nt, nl, tlo);
