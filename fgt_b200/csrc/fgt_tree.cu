@@ -397,8 +397,11 @@ void tree_build(Tree& t, int dim, int iperiod, int npwlevel, int ndiv, double bs
   if (nt > 0) launch_point_keys(dim, d_trg, nt, kp, tkey, s);
   // Source counts per box come from a dense histogram of the full keys
   // (prefix sums over the 2^(dim*D) finest cells) when the key space is
-  // small enough, else from binary searches in the sorted keys.
-  const bool dense = dim * D <= 24;
+  // small, and not much larger than the point set (clearing and scanning
+  // 2^24 cells costs ~0.3 ms, far more than sorting a few thousand keys),
+  // else from binary searches in the sorted keys.
+  const bool dense =
+      dim * D <= 24 && (1ll << (dim * D)) <= 4ll * ((long long)ns + nt) + (1ll << 18);
   DBuf<int> cellsum;
   if (dense) {
     const int ncell = 1 << (dim * D);
