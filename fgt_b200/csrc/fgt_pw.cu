@@ -20,6 +20,7 @@ struct FormIO {
   const WorkItem* items;  // form items, most sources first
   const int* n_items;     // item count (device)
   int max_items;          // upper bound of the item count (grid sizing)
+  int slab, nslab;        // x-slab grids: planes per slab and slabs per box (1: whole grids)
   int* next;              // work counter (zero at launch)
 };
 
@@ -470,6 +471,133 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
   }
 }
 
+// ------------------------------------------------------ x-slab grids (3D)
+// A grid too large for shared memory (eps <= 1e-9 with plane waves) is cut
+// into slabs of whole x-planes (slab_plan).  A work item is (box, point part,
+// slab); its CTA holds the slab in shared memory, spreads every point of its
+// part into the planes that the point's stencil shares with the slab
+// (shared-memory atomics), runs the z and y passes of the form on the slab's
+// planes (they never leave an x-plane), and adds the slab's terms of the x
+// transform, times the weights of the expansion, to the box's expansion with
+// global atomics (the expansions are zeroed before the launch).  No grid
+// leaves shared memory; the slabs of a box run on different SMs.
+
+// Spread one point into the planes [x0, x1) of a slab (plane xl of the slab
+// is grid plane x0 + xl).
+template <typename T, int W>
+__device__ __forceinline__ void spread_point_slab(const PWArgs<T>& a, T* B, const double* x, T str,
+                                                  int x0, int x1) {
+  const Geo& g = a.g;
+  T ph[2][W];  // y and z rows; the x values are computed as the x loop reaches them
+  int b[3];
+  T f0x;
+  b[0] = kernel_start<T>(a, x[0], f0x) - g.l0;
+  b[1] = kernel_row<T, W>(a, x[1], ph[0]) - g.l0;
+  b[2] = kernel_row<T, W>(a, x[2], ph[1]) - g.l0;
+#pragma unroll
+  for (int d = 0; d < 3; d++) b[d] = b[d] < 0 ? 0 : (b[d] > g.G - W ? g.G - W : b[d]);
+  const int jlo = max(0, x0 - b[0]), jhi = min(W, x1 - b[0]);
+  T* by = B + b[1] * g.str[1] + b[2];
+#pragma unroll 1
+  for (int jx = jlo; jx < jhi; jx++) {
+    T* bx = by + (b[0] + jx - x0) * g.str[0];
+    const T vx = str * es_kernel<T>((f0x + (T)jx) * a.inv_hw, a.beta);
+#pragma unroll
+    for (int jy = 0; jy < W; jy++) {
+      T* bxy = bx + jy * g.str[1];
+      const T vxy = vx * ph[0][jy];
+#pragma unroll
+      for (int jz = 0; jz < W; jz++) atomicAdd(bxy + jz, vxy * ph[1][jz]);
+    }
+  }
+}
+
+template <typename T, int W>
+__global__ void __launch_bounds__(PW_THREADS) k_form_slab(PWArgs<T> a, FormIO io, FormPtrs<T> p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Geo& g = a.g;
+  const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int NFp = pad4(NF), NHp = pad4(NH);
+  const T* twf = stage_tw(sm, a.twf, 2 * G * NFp);
+  const T* twh = stage_tw(sm + 2 * G * NFp, a.twh, 2 * G * NHp);
+  int* ordtmp = reinterpret_cast<int*>(sm + tw_elems_t<T>(G, K));  // ORDER_CHUNK
+  int* ordcnt = ordtmp + ORDER_CHUNK;                               // 32
+  unsigned short* perm = reinterpret_cast<unsigned short*>(ordcnt + 32);  // ORDER_CHUNK
+  T* B = reinterpret_cast<T*>(smem_raw + order_offset<T>(G, K));  // io.slab planes
+  const int C = io.nslab, nline = NF * NH;
+  __syncthreads();
+  __shared__ int s_next;
+  const int n_items = *io.n_items;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_next = atomicAdd(io.next, 1);
+    __syncthreads();
+    if (s_next >= n_items) break;
+    const WorkItem it = io.items[s_next];
+    const int fb = it.slot;
+    if (!FGT_DCHECK(fb >= 0 && fb < io.n_form && it.nparts % C == 0, 206)) continue;
+    const int box = io.form_box[fb];
+    const int x0 = (it.part % C) * io.slab, x1 = min(G, x0 + io.slab), np_ = x1 - x0;
+    int p0, p1;
+    part_range(io.s_lo[box], io.s_hi[box], it.part / C, it.nparts / C, p0, p1);
+    if (!FGT_DCHECK(p0 >= 0 && p0 <= p1 && p1 <= io.ns && np_ > 0 && np_ <= io.slab, 207))
+      continue;
+    for (int id = 0; id < io.nd; id++) {
+      T* mp = p.mp + ((size_t)fb * io.nd + id) * 2 * g.nexp;
+      for (int comp = 0; comp < io.ncomp; comp++) {
+        const bool is_q = io.has_q && comp == 0;
+        const int dd = is_q ? -1 : comp - io.has_q;
+        for (int i = threadIdx.x; i < np_ * g.str[0]; i += blockDim.x) B[i] = T(0);
+        __syncthreads();
+        for (int c0 = p0; c0 < p1; c0 += ORDER_CHUNK) {
+          const int n = min(ORDER_CHUNK, p1 - c0);
+          order_chunk<T, 3, W>(a, p.off, io.ns, c0, n, perm, ordtmp, ordcnt);
+          for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int pt = c0 + perm[i];
+            double x[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) x[k] = p.off[(size_t)k * io.ns + pt] * a.scale_d;
+            const T str = is_q ? p.q[(size_t)id * io.ns + pt]
+                               : p.ds[(size_t)id * io.ns + pt] * p.rn[(size_t)dd * io.ns + pt];
+            spread_point_slab<T, W>(a, B, x, str, x0, x1);
+          }
+          __syncthreads();
+        }
+        // passes along z (real -> half complex) and y on the slab's planes
+        pass_inplace<T, 0>(B, np_ * G, G, g.str[0], g.str[1], 1, 2, G, NH, twh);
+        pass_inplace<T, 1>(B, np_ * NH, NH, g.str[0], 2, g.str[1], g.str[1], G, NF, twf);
+        // the slab's terms of the x transform, weights and deconvolution
+        // (as k_form's expansion step), added to the box's expansion
+        for (int o = threadIdx.x; o < NF * nline; o += blockDim.x) {
+          const int kxi = o / nline, line = o - kxi * nline;
+          const int kyi = line / NH, kz = line - kyi * NH;
+          const T* bl = B + kyi * g.str[1] + 2 * kz;
+          const T* tw = twf + (size_t)x0 * 2 * NFp + kxi;
+          T re = T(0), im = T(0);
+          for (int xl = 0; xl < np_; xl++, bl += g.str[0], tw += 2 * NFp) {
+            const T br = bl[0], bi = bl[1], tr = tw[0], ti = tw[NFp];
+            re += br * tr - bi * ti;
+            im += br * ti + bi * tr;
+          }
+          const int ki[3] = {kxi, kyi, kz + K};
+          const T f = a.facf[ki[0]] * a.facf[ki[1]] * a.facf[ki[2]];
+          T vr = re * f, vi = im * f;
+          if (!is_q) {  // * (-i) ts(k_d) / sqrt(delta0)
+            const T cc = a.ts[sel3(ki, dd)] * a.inv_sqd0;
+            const T tr = vi * cc, ti = -vr * cc;
+            vr = tr;
+            vi = ti;
+          }
+          atomicAdd(mp + 2 * o, vr);
+          atomicAdd(mp + 2 * o + 1, vi);
+        }
+        __syncthreads();
+      }
+    }
+  }
+}
+
 // Form of small 2D boxes, one warp per box (see small2_layout): the boxes
 // order[first..n_form) of the longest-processing-time order, which all hold
 // at most SMALL2_MAX sources.  Same sums as k_form for DIM = 2.
@@ -741,6 +869,12 @@ int launch_form(PWArgs<T>& a, const FormIO& io, const FormPtrs<T>& fp, DBuf<T>& 
     auto k = k_form<T, DIM, W, false, false>;
     set_smem(k, need);
     k<<<grid, PW_THREADS, need, s>>>(a, io, fp);
+  } else if (DIM == 3 && io.nslab > 1) {
+    // x-slab grids (the expansions were zeroed by the caller)
+    const size_t sm = fix + sizeof(T) * (size_t)a.g.str[0] * io.slab;
+    auto k = k_form_slab<T, W>;
+    set_smem(k, sm);
+    k<<<grid, PW_THREADS, sm, s>>>(a, io, fp);
   } else {
     gs.alloc((size_t)grid * a.g.bufsz, s);
     a.gscratch = gs;
@@ -978,12 +1112,23 @@ int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>
     k_first_at_most<<<1, 32, 0, s>>>(okey, L.n_form, SMALL2_MAX, first);
     FGT_LAUNCH_CHECK();
   }
+  // FP32 grids too large for shared memory: x-slabs (3D without
+  // wrap-around).  FP64 keeps the global-memory grid: its shared-memory
+  // atomics are no faster than global ones (the slab form of the FP64
+  // eps = 1e-9 cell took 101 ms against 88 ms).
+  SlabPlan sp;
+  if (sizeof(T) == 4 &&
+      sizeof(T) * (size_t)a.g.bufsz + order_offset<T>(a.g.G, a.g.K) > (size_t)MAXSMEM)
+    sp = slab_plan(a.g, sizeof(T), order_offset<T>(a.g.G, a.g.K));
+  if (sp.nslab > 1) D.mp.zero();
   ItemList il;
   build_items(il, L.n_form, small2 ? first.get() : nullptr, oval, L.form_box, src.lo, src.hi,
-              nullptr, nullptr, src.n, thr, true, s);
+              nullptr, nullptr, src.n, thr, true, s, sp.nslab);
   io.items = il.items;
   io.n_items = il.n_items;
   io.max_items = il.max_items;
+  io.slab = sp.planes;
+  io.nslab = sp.nslab;
   io.next = next;
   FormPtrs<T> fp;
   fp.off = src.off;

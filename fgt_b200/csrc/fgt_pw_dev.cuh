@@ -891,13 +891,15 @@ struct SplitRec {
 };
 
 // Part count of entry i of a sorted slot list (entries at or beyond *count
-// get 0): ceil(points / thr) when the box holds more than thr points, else 1.
-// nsplit[i] = part count of split boxes, 0 otherwise.
+// get 0): ceil(points / thr) point parts when the box holds more than thr
+// points, else 1, times nslab grid slabs (x-slab grids: every part of a box
+// spreads or interpolates into one slab).  nsplit[i] = part count of boxes
+// split into point parts with partial expansions (no slabs), 0 otherwise.
 __global__ void k_item_parts(int n, const int* __restrict__ count, const uint32_t* __restrict__ order,
                              const int* __restrict__ box, const int* __restrict__ lo0,
                              const int* __restrict__ hi0, const int* __restrict__ lo1,
-                             const int* __restrict__ hi1, int thr, int* __restrict__ nparts,
-                             int* __restrict__ nsplit) {
+                             const int* __restrict__ hi1, int thr, int nslab,
+                             int* __restrict__ nparts, int* __restrict__ nsplit) {
   const int m = count ? *count : n;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int np = 0;
@@ -907,17 +909,19 @@ __global__ void k_item_parts(int n, const int* __restrict__ count, const uint32_
           (long long)(hi0[b] - lo0[b]) + (lo1 ? (long long)(hi1[b] - lo1[b]) : 0);
       np = c > thr ? (int)((c + thr - 1) / thr) : 1;
     }
-    nparts[i] = np;
-    nsplit[i] = np > 1 ? np : 0;
+    nparts[i] = np * nslab;
+    nsplit[i] = (nslab == 1 && np > 1) ? np : 0;
   }
 }
 
 // Items of every entry (offsets from exclusive scans of nparts and nsplit);
 // split boxes are also listed in `split` (order of the list unspecified; each
-// record carries its own slots, so results do not depend on it).
+// record carries its own slots, so results do not depend on it).  With
+// nslab > 1, part p is slab p % nslab of point part p / nslab, and no item
+// has a partial slot (the slab kernels add into the box's expansion).
 __global__ void k_item_fill(int n, const int* __restrict__ count, const uint32_t* __restrict__ order,
                             const int* __restrict__ nparts, const int* __restrict__ ioff,
-                            const int* __restrict__ poff, WorkItem* __restrict__ items,
+                            const int* __restrict__ poff, int nslab, WorkItem* __restrict__ items,
                             SplitRec* __restrict__ split, int* __restrict__ nsplit_total) {
   const int m = count ? *count : n;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
@@ -927,10 +931,10 @@ __global__ void k_item_fill(int n, const int* __restrict__ count, const uint32_t
       w.slot = slot;
       w.part = p;
       w.nparts = np;
-      w.pslot = np > 1 ? poff[i] + p : -1;
+      w.pslot = (nslab == 1 && np > 1) ? poff[i] + p : -1;
       items[o + p] = w;
     }
-    if (np > 1 && split) {
+    if (nslab == 1 && np > 1 && split) {
       const int k = atomicAdd(nsplit_total, 1);
       SplitRec r;
       r.slot = slot;
@@ -955,7 +959,8 @@ inline int eval_split_threshold(long long n) {
 // Work items of a sorted slot list (host side, all sizes stay on the device).
 // n: list length bound; count: actual length on the device (or null = n);
 // npts_bound: upper bound of the points over all listed boxes; thr: split
-// threshold.  Items and split records live in the call's workspace.
+// threshold; nslab: grid slabs per box (1: whole grids).  Items and split
+// records live in the call's workspace.
 struct ItemList {
   DBuf<WorkItem> items;
   DBuf<SplitRec> split;
@@ -965,11 +970,11 @@ struct ItemList {
 inline void build_items(ItemList& il, int n, const int* count, const uint32_t* order,
                         const int* box, const int* lo0, const int* hi0, const int* lo1,
                         const int* hi1, long long npts_bound, int thr, bool want_split,
-                        cudaStream_t s) {
+                        cudaStream_t s, int nslab = 1) {
   // every split box holds more than thr points and has at most 2*points/thr
   // parts; every other box has one
   const long long extra = 2 * (npts_bound / std::max(thr, 1)) + 1;
-  il.max_items = (int)std::min<long long>((long long)n + extra, 1ll << 30);
+  il.max_items = (int)std::min<long long>(((long long)n + extra) * nslab, 1ll << 30);
   il.max_partial = (int)std::min<long long>(extra, 1ll << 30);
   DBuf<int> np(std::max(n, 1), s), ns(std::max(n, 1), s), ioff(std::max(n, 1), s),
       poff(std::max(n, 1), s);
@@ -984,14 +989,35 @@ inline void build_items(ItemList& il, int n, const int* count, const uint32_t* o
     il.n_partial.zero();
     return;
   }
-  k_item_parts<<<grid_for(n, 256), 256, 0, s>>>(n, count, order, box, lo0, hi0, lo1, hi1, thr, np,
-                                                 ns);
+  k_item_parts<<<grid_for(n, 256), 256, 0, s>>>(n, count, order, box, lo0, hi0, lo1, hi1, thr,
+                                                 nslab, np, ns);
   FGT_LAUNCH_CHECK();
   exclusive_scan_i32(np, ioff, n, il.n_items, s);
   exclusive_scan_i32(ns, poff, n, il.n_partial, s);
-  k_item_fill<<<grid_for(n, 256), 256, 0, s>>>(n, count, order, np, ioff, poff, il.items,
+  k_item_fill<<<grid_for(n, 256), 256, 0, s>>>(n, count, order, np, ioff, poff, nslab, il.items,
                                                 want_split ? il.split.get() : nullptr, il.n_split);
   FGT_LAUNCH_CHECK();
+}
+
+// x-slab grids (3D, no wrap-around): a grid too large for shared memory is
+// cut into nslab slabs of at most `planes` whole x-planes (each plane holds
+// str[0] elements), sized so that `fixed` bytes of scratch plus one slab fit
+// in SLAB_SMEM bytes of shared memory.  The passes along z and y stay inside
+// an x-plane; only the x transform and the stencils' x extent cross slabs.
+constexpr size_t SLAB_SMEM = 216 * 1024;
+struct SlabPlan {
+  int planes = 0, nslab = 1;
+  size_t smem = 0;
+};
+inline SlabPlan slab_plan(const Geo& g, size_t tsize, size_t fixed) {
+  SlabPlan r;
+  const size_t plane = tsize * (size_t)g.str[0];
+  if (g.dim != 3 || g.wrap || fixed + plane > SLAB_SMEM) return r;
+  const int pmax = (int)((SLAB_SMEM - fixed) / plane);
+  r.nslab = (g.G + pmax - 1) / pmax;
+  r.planes = (g.G + r.nslab - 1) / r.nslab;
+  r.smem = fixed + plane * (size_t)r.planes;
+  return r;
 }
 
 // Point range [q0, q1) of part `part` of `nparts` of [lo, hi).

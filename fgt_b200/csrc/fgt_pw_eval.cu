@@ -32,6 +32,7 @@ struct EvalPtrs {
   int n[2], ncomp[2];
   int nd, ncomp_max;
   int cell_bins;  // base cells of the sub-grid for the cell order, 0: bank-class order
+  int slab, nslab;  // x-slab grids: planes per slab and slabs per box (1: whole grids)
 };
 
 // component factor (complex) of evaluation component c at mode ki[]
@@ -236,6 +237,242 @@ __global__ void __launch_bounds__(eval_threads<T, DIM, W, GB, DERIV>())
               } else {
                 const T v = interp_point<T, DIM, W>(a, BV, x);
                 atomicAdd(&outs[((size_t)c * p.nd + id) * ne + pt], (double)v);
+              }
+            }
+            __syncthreads();
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------ x-slab grids (3D)
+// A grid too large for shared memory is cut into slabs of whole x-planes
+// (slab_plan).  A work item is (box, point part, slab); its CTA computes the
+// slab's planes of the box's grid from the local expansion (the x transform
+// evaluated at those planes only, reading the expansion from global
+// memory), runs the y and z passes on them (they never leave an x-plane),
+// and adds to every point of its part the terms of the interpolation that
+// fall on the slab's planes; a point's outputs are the sum of its slabs'
+// terms (global atomics, as for the parts of split boxes).
+
+// Sums over stencil cells [jlo, jhi) of one coordinate of the kernel values
+// and of their derivatives, in FP64: the function of es_kernel / kernel_val_d
+// with the launch's parameters (the same kernel as the T arithmetic), at
+// FP64 offsets.
+template <typename T>
+__device__ __forceinline__ void kernel_sums_d(const PWArgs<T>& a, double x, int jlo, int jhi,
+                                              double& ks, double& kd) {
+  const double u = x * a.inv_dx_d;
+  const double f0 = ceil(u - a.hwdx_d) - u;
+  const double ih = (double)a.inv_hw, be = (double)a.beta, bds = be * (double)a.dscale;
+  ks = 0.0;
+  kd = 0.0;
+  for (int j = jlo; j < jhi; j++) {
+    const double z = (f0 + (double)j) * ih;
+    const double q = 1.0 - z * z;
+    const double r = q > 0.0 ? sqrt(q) : 0.0;
+    const double e = exp(-be * (z * z) / (1.0 + r));
+    ks += e;
+    kd += q > 0.0 ? e * bds * z / r : 0.0;
+  }
+}
+
+// Interpolation terms of one point on the planes [x0, x1) of a slab (slab
+// plane xl is grid plane x0 + xl).  DERIV: potential and gradient as
+// interp_grad_cells, with the centre cell of the slab's share of the stencil
+// as the reference value bref: the T sums run over B - bref and bref's own
+// terms (bref times products of kernel and derivative sums) are added back in
+// FP64, where a slab's share of the x derivatives, unlike the whole
+// stencil's, does not sum to ~0.  Else the potential of one component grid.
+// Returns false when the stencil misses the slab.
+template <typename T, int W, bool DERIV>
+__device__ __forceinline__ bool interp_slab(const PWArgs<T>& a, const T* B, const double* x,
+                                            int x0, int x1, double* v) {
+  const Geo& g = a.g;
+  T f0x;
+  int bx = kernel_start<T>(a, x[0], f0x) - g.l0;
+  bx = bx < 0 ? 0 : (bx > g.G - W ? g.G - W : bx);
+  const int jlo = max(0, x0 - bx), jhi = min(W, x1 - bx);
+  if (jlo >= jhi) return false;
+  int b1, b2;
+  if constexpr (DERIV) {
+    T ph[2][W], dph[2][W];  // y and z rows
+    b1 = kernel_row_d<T, W>(a, x[1], ph[0], dph[0]) - g.l0;
+    b2 = kernel_row_d<T, W>(a, x[2], ph[1], dph[1]) - g.l0;
+    b1 = b1 < 0 ? 0 : (b1 > g.G - W ? g.G - W : b1);
+    b2 = b2 < 0 ? 0 : (b2 > g.G - W ? g.G - W : b2);
+    const T* row0 = B + b1 * g.str[1] + b2;
+    const int jm = (jlo + jhi) / 2;
+    const T bref = row0[(bx + jm - x0) * g.str[0] + (W / 2) * g.str[1] + W / 2];
+    // kernel sums and derivative sums of the three rows (x: the slab's share)
+    T ksy = T(0), ksz = T(0), ksx = T(0), kdx = T(0), kdy = T(0), kdz = T(0);
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+      ksy += ph[0][j];
+      ksz += ph[1][j];
+      kdy += dph[0][j];
+      kdz += dph[1][j];
+    }
+    T pot = T(0), gx = T(0), gy = T(0), gz = T(0);
+#pragma unroll 1
+    for (int jx = jlo; jx < jhi; jx++) {
+      T px, dpx;
+      kernel_val_d<T>(a, f0x, jx, px, dpx);
+      ksx += px;
+      kdx += dpx;
+      const T* rx = row0 + (bx + jx - x0) * g.str[0];
+      T t0 = T(0), t1 = T(0), t2 = T(0);
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        const T* ln = rx + jy * g.str[1];
+        T s0 = T(0), s1 = T(0);
+#pragma unroll
+        for (int jz = 0; jz < W; jz++) {
+          const T bv = ln[jz] - bref;
+          s0 += bv * ph[1][jz];
+          s1 += bv * dph[1][jz];
+        }
+        t0 += ph[0][jy] * s0;
+        t1 += dph[0][jy] * s0;
+        t2 += ph[0][jy] * s1;
+      }
+      pot += px * t0;
+      gx += dpx * t0;
+      gy += px * t1;
+      gz += px * t2;
+    }
+    double Kx, Dx, Ky, Dy, Kz, Dz;
+    if constexpr (std::is_same<T, double>::value) {
+      Kx = ksx; Dx = kdx; Ky = ksy; Dy = kdy; Kz = ksz; Dz = kdz;
+    } else {
+      kernel_sums_d<T>(a, x[0], jlo, jhi, Kx, Dx);
+      kernel_sums_d<T>(a, x[1], 0, W, Ky, Dy);
+      kernel_sums_d<T>(a, x[2], 0, W, Kz, Dz);
+    }
+    const double br = (double)bref;
+    v[0] = (double)pot + br * (Kx * Ky * Kz);
+    v[1] = (double)gx + br * (Dx * Ky * Kz);
+    v[2] = (double)gy + br * (Kx * Dy * Kz);
+    v[3] = (double)gz + br * (Kx * Ky * Dz);
+  } else {
+    T ph[2][W];
+    b1 = kernel_row<T, W>(a, x[1], ph[0]) - g.l0;
+    b2 = kernel_row<T, W>(a, x[2], ph[1]) - g.l0;
+    b1 = b1 < 0 ? 0 : (b1 > g.G - W ? g.G - W : b1);
+    b2 = b2 < 0 ? 0 : (b2 > g.G - W ? g.G - W : b2);
+    const T* row0 = B + b1 * g.str[1] + b2;
+    T acc = T(0);
+#pragma unroll 1
+    for (int jx = jlo; jx < jhi; jx++) {
+      const T px = es_kernel<T>((f0x + (T)jx) * a.inv_hw, a.beta);
+      const T* rx = row0 + (bx + jx - x0) * g.str[0];
+      T sx = T(0);
+#pragma unroll
+      for (int jy = 0; jy < W; jy++) {
+        const T* ln = rx + jy * g.str[1];
+        T sy = T(0);
+#pragma unroll
+        for (int jz = 0; jz < W; jz++) sy += ln[jz] * ph[1][jz];
+        sx += sy * ph[0][jy];
+      }
+      acc += sx * px;
+    }
+    v[0] = (double)acc;
+  }
+  return true;
+}
+
+template <typename T, int W, bool DERIV>
+__global__ void __launch_bounds__(PW_THREADS) k_eval_slab(PWArgs<T> a, EvalPtrs<T> p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Geo& g = a.g;
+  const int K = g.K, NF = 2 * K + 1, NH = K + 1, G = g.G;
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int Gp = pad4(G);
+  const T* tif = stage_tw(sm, a.tif, 2 * NF * Gp);
+  const T* tih = stage_tw(sm + 2 * NF * Gp, a.tih, 2 * NH * Gp);
+  int* ordtmp = reinterpret_cast<int*>(sm + tw_elems_t<T>(G, K));       // ORDER_CHUNK
+  int* ordcnt = ordtmp + ORDER_CHUNK;                                    // 32
+  unsigned short* perm = reinterpret_cast<unsigned short*>(ordcnt + 32);  // ORDER_CHUNK
+  T* B = reinterpret_cast<T*>(smem_raw + order_offset<T>(G, K));       // p.slab planes
+  const int C = p.nslab, nline = NF * NH;
+  __syncthreads();
+  __shared__ int s_next;
+  const int n_items = *p.n_items;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_next = atomicAdd(p.next, 1);
+    __syncthreads();
+    if (s_next >= n_items) break;
+    const WorkItem it = p.items[s_next];
+    const int e = it.slot;
+    if (!FGT_DCHECK(e >= 0 && e < p.nbox && it.nparts % C == 0, 305)) continue;
+    const int box = p.eval_box[e];
+    const int x0 = (it.part % C) * p.slab, x1 = min(G, x0 + p.slab), np_ = x1 - x0;
+    if (!FGT_DCHECK(np_ > 0 && np_ <= p.slab, 306)) continue;
+    for (int id = 0; id < p.nd; id++) {
+      const T* L = p.loc + ((size_t)e * p.nd + id) * 2 * g.nexp;
+      for (int c = 0; c < (DERIV ? 1 : p.ncomp_max); c++) {
+        // the x transform at the slab's planes (factors as build_eval_grid)
+        for (int o = threadIdx.x; o < np_ * nline; o += blockDim.x) {
+          const int xl = o / nline, line = o - xl * nline;
+          const int kyi = line / NH, kz = line - kyi * NH;
+          const T fyz = a.faci[kyi] * a.faci[kz + K];
+          const T* tw = tif + x0 + xl;
+          T re = T(0), im = T(0);
+          for (int kx = 0; kx < NF; kx++, tw += 2 * Gp) {
+            const int m = kx * nline + line;
+            const int ki[3] = {kx, kyi, kz + K};
+            T fr, fi;
+            eval_factor<T, 3>(a, c, ki, fr, fi);
+            const T f = a.faci[kx] * fyz;
+            fr *= f;
+            fi *= f;
+            const T lr = L[2 * m], li = L[2 * m + 1];
+            const T vr = lr * fr - li * fi, vi = lr * fi + li * fr;
+            const T tr = tw[0], ti = tw[Gp];
+            re += vr * tr - vi * ti;
+            im += vr * ti + vi * tr;
+          }
+          T* bo = B + xl * g.str[0] + kyi * g.str[1] + 2 * kz;
+          bo[0] = re;
+          bo[1] = im;
+        }
+        __syncthreads();
+        pass_inplace<T, 1>(B, np_ * NH, NH, g.str[0], 2, g.str[1], g.str[1], NF, G, tif);
+        pass_inplace<T, 2>(B, np_ * G, G, g.str[0], g.str[1], 2, 1, NH, G, tih);
+        for (int set = 0; set < 2; set++) {
+          const int ne = set ? p.n[1] : p.n[0];
+          if (c >= (set ? p.ncomp[1] : p.ncomp[0]) || ne == 0) continue;
+          const double* offs = set ? p.off[1] : p.off[0];
+          double* outs = set ? p.out[1] : p.out[0];
+          const int nc = set ? p.ncomp[1] : p.ncomp[0];
+          int q0, q1;
+          part_range(set ? p.lo[1][box] : p.lo[0][box], set ? p.hi[1][box] : p.hi[0][box],
+                     it.part / C, it.nparts / C, q0, q1);
+          if (!FGT_DCHECK(q0 >= 0 && q0 <= q1 && q1 <= ne, 307)) continue;
+          for (int c0 = q0; c0 < q1; c0 += ORDER_CHUNK) {
+            const int n = min(ORDER_CHUNK, q1 - c0);
+            order_chunk<T, 3, W>(a, offs, ne, c0, n, perm, ordtmp, ordcnt);
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+              const int pt = c0 + perm[i];
+              double x[3];
+#pragma unroll
+              for (int k = 0; k < 3; k++) x[k] = offs[(size_t)k * ne + pt] * a.scale_d;
+              double v[4];
+              if (!interp_slab<T, W, DERIV>(a, B, x, x0, x1, v)) continue;
+              if constexpr (DERIV) {
+                atomicAdd(&outs[(size_t)id * ne + pt], v[0]);
+                if (nc > 1) {
+#pragma unroll
+                  for (int d = 0; d < 3; d++)
+                    atomicAdd(&outs[((size_t)(1 + d) * p.nd + id) * ne + pt], v[1 + d]);
+                }
+              } else {
+                atomicAdd(&outs[((size_t)c * p.nd + id) * ne + pt], v[0]);
               }
             }
             __syncthreads();
@@ -698,6 +935,16 @@ int launch_eval_k(PWArgs<T>& a, const EvalPtrs<T>& ep, DBuf<T>& gs, cudaStream_t
     epk.cell_bins =
         (sizeof(T) == 4 && !a.g.wrap && nb > 0 && padded <= NBINS_MAX) ? (int)nbins : 0;
   }
+  if constexpr (DIM == 3) {
+    if (gb && ep.nslab > 1) {  // x-slab grids
+      const size_t ss = order_offset<T>(a.g.G, a.g.K) + sizeof(T) * (size_t)a.g.str[0] * ep.slab;
+      auto k = k_eval_slab<T, W, DERIV>;
+      set_smem(k, ss);
+      k<<<grid, PW_THREADS, ss, s>>>(a, epk);
+      FGT_LAUNCH_CHECK();
+      return 1;
+    }
+  }
   if (gb) {
     gs.alloc((size_t)grid * a.g.bufsz, s);
     a.gscratch = gs;
@@ -867,6 +1114,12 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   ep.items = nullptr;
   ep.n_items = nullptr;
   ep.max_items = 0;
+  // grids too large for shared memory: x-slabs (3D without wrap-around)
+  SlabPlan sp;
+  if (eval_offset<T>(a.g.G, a.g.K) + sizeof(T) * (size_t)a.g.bufsz > (size_t)MAXSMEM)
+    sp = slab_plan(a.g, sizeof(T), order_offset<T>(a.g.G, a.g.K));
+  ep.slab = sp.planes;
+  ep.nslab = sp.nslab;
   ItemList il;
   DBuf<int> first2(1, s), next2(1, s);
   DBuf<T> gs;
@@ -901,7 +1154,8 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
     build_items(il, L.n_eval, small2 ? first2.get() : counts.get(),
                 reinterpret_cast<const uint32_t*>(lbig.get()),
                 L.eval_box, u0 ? e0.lo : e1.lo, u0 ? e0.hi : e1.hi, (u0 && u1) ? e1.lo : nullptr,
-                (u0 && u1) ? e1.hi : nullptr, npts, eval_split_threshold(npts), false, s);
+                (u0 && u1) ? e1.hi : nullptr, npts, eval_split_threshold(npts), false, s,
+                sp.nslab);
     ep.items = il.items;
     ep.n_items = il.n_items;
     ep.max_items = il.max_items;
