@@ -49,6 +49,7 @@ class FgtStats(C.Structure):
         ("pts_form", C.c_double), ("pts_eval_nufft", C.c_double),
         ("pts_eval_modal", C.c_double), ("bs0", C.c_double), ("cen0", C.c_double * 3),
         ("ms", C.c_double * 12), ("small_eval_used", C.c_int), ("tuned", C.c_int),
+        ("slabs_form", C.c_int), ("slabs_eval", C.c_int),
     ]
 
     def as_dict(self):

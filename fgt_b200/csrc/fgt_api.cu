@@ -634,6 +634,8 @@ void execute(const Setup& u, const Call& c, const fgt_opts& o, fgt_stats* st, cu
     st->pts_form = work.pts_form;
     st->pts_eval_nufft = work.pts_nufft;
     st->pts_eval_modal = work.pts_modal;
+    st->slabs_form = work.slabs_form;
+    st->slabs_eval = work.slabs_eval;
     {
       // near-field pair arithmetic (charge: 12 pot, 21 +grad, 21+5*nhess +hess)
       auto per = [&](int pgh) {

@@ -1121,6 +1121,7 @@ int pw_form(const PWParams& P, const Tree& t, const Lists& L, const SourceSet<T>
       sizeof(T) * (size_t)a.g.bufsz + order_offset<T>(a.g.G, a.g.K) > (size_t)MAXSMEM)
     sp = slab_plan(a.g, sizeof(T), order_offset<T>(a.g.G, a.g.K));
   if (sp.nslab > 1) D.mp.zero();
+  if (work) work->slabs_form = sp.nslab;
   ItemList il;
   build_items(il, L.n_form, small2 ? first.get() : nullptr, oval, L.form_box, src.lo, src.hi,
               nullptr, nullptr, src.n, thr, true, s, sp.nslab);

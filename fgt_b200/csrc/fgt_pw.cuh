@@ -54,6 +54,7 @@ struct PWWork {
   double pts_form = 0, pts_nufft = 0, pts_modal = 0;
   double flops_form = 0, flops_eval = 0, bytes_translate = 0;
   int n_nufft = 0, w_eval = 0, G_eval = 0;
+  int slabs_form = 1, slabs_eval = 1;  // x-slabs per sub-grid (1: whole grids)
 };
 
 // Forms the expansions of all form boxes.  Returns launches.

@@ -1120,6 +1120,7 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
     sp = slab_plan(a.g, sizeof(T), order_offset<T>(a.g.G, a.g.K));
   ep.slab = sp.planes;
   ep.nslab = sp.nslab;
+  if (work) work->slabs_eval = sp.nslab;
   ItemList il;
   DBuf<int> first2(1, s), next2(1, s);
   DBuf<T> gs;

@@ -66,6 +66,8 @@ typedef struct fgt_stats {
   double ms[12];
   int small_eval_used;   /* modal-evaluation threshold the call used */
   int tuned;             /* 1: parameters came from the tuning cache or a tuning run */
+  int slabs_form;        /* x-slabs per form sub-grid (1: whole grids) */
+  int slabs_eval;        /* x-slabs per evaluation sub-grid (1: whole grids) */
 } fgt_stats;
 
 typedef struct fgt_opts {

@@ -114,6 +114,7 @@ def _benchmark_regime_cases():
 
 
 CASES = _case_list()
+SLAB_CASES = ("3d_eps1e-9", "3d_hess_dipole_eps1e-9", "3d_eps1e-12", "config2_clusters_eps1e-9")
 _ORACLE = {}
 
 
@@ -136,6 +137,11 @@ def test_pfgt_matches_oracle(fgt, oracle, case, prec):
                 "config3_periodic_nd4",
                 "config5_delta1e-1_root", "config5_delta1e-1_eps1e-3"):
         assert r["stats"]["n_form_boxes"] > 0, (name, r["stats"])  # the plane-wave path ran
+    if name in SLAB_CASES:
+        # 3D grids beyond shared memory: evaluated in x-slabs; formed in
+        # x-slabs in FP32 (FP64 forms keep a global-memory grid)
+        assert r["stats"]["slabs_eval"] > 1, (name, r["stats"])
+        assert (r["stats"]["slabs_form"] > 1) == (prec == "mixed"), (name, r["stats"])
     # mixed: FP32 bulk arithmetic resolves about 1e-6 (below eps = 1e-6,
     # outside the precision policy, the W^3 = 1728-2744 cell stencils of the
     # eps = 1e-9 / 1e-12 kernels land at 1-2e-6 on some point sets)
