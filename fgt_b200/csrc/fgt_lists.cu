@@ -345,26 +345,40 @@ void build_lists(const Tree& t, int npwlevel, int iperiod0, int nlevend, bool do
                  cudaStream_t s) {
   TV tv = make_tv(t, npwlevel, iperiod0, nlevend);
   int nb = t.nboxes;
-  // direct near field
+  // direct near field: list lengths; the plane-wave box flags are counted
+  // before the one read-back of all three totals
   L.l1_ptr.alloc(nb + 1, s);
-  {
-    DBuf<int> cnt(nb, s), tot(1, s);
-    launch_list1<false>(tv, nb, cnt, nullptr, nullptr, s);
-    exclusive_scan_i32(cnt, L.l1_ptr, nb, L.l1_ptr.get() + nb, s);
-    L.n_l1 = fetch_int(L.l1_ptr.get() + nb, s);
-    L.l1_src.alloc(std::max(L.n_l1, 1), s);
-    launch_list1<true>(tv, nb, nullptr, L.l1_ptr, L.l1_src, s);
-  }
+  DBuf<int> cnt1(nb, s);
+  launch_list1<false>(tv, nb, cnt1, nullptr, nullptr, s);
+  exclusive_scan_i32(cnt1, L.l1_ptr, nb, L.l1_ptr.get() + nb, s);
   L.n_form = L.n_eval = L.n_trans = 0;
+  const int lo = do_pw ? t.lev_start[t.ncutoff] : 0;
+  const int n = do_pw ? t.lev_start[t.ncutoff + 1] - lo : 0;
+  DBuf<int> ff, fe, pf, pe, tf, te, fslot;
+  if (do_pw) {
+    ff.alloc(n, s);
+    fe.alloc(n, s);
+    pf.alloc(n, s);
+    pe.alloc(n, s);
+    tf.alloc(1, s);
+    te.alloc(1, s);
+    fslot.alloc(n, s);
+    k_pw_flags<<<grid_for(n, 128), 128, 0, s>>>(tv, t.ndiv, ff, fe);
+    FGT_LAUNCH_CHECK();
+    exclusive_scan_i32(ff, pf, n, tf, s);
+    exclusive_scan_i32(fe, pe, n, te, s);
+  }
+  {
+    const int* src[3] = {L.l1_ptr.get() + nb, tf.get(), te.get()};
+    int h[3] = {0, 0, 0};
+    fetch_ints(src, do_pw ? 3 : 1, h, s);
+    L.n_l1 = h[0];
+    L.n_form = h[1];
+    L.n_eval = h[2];
+  }
+  L.l1_src.alloc(std::max(L.n_l1, 1), s);
+  launch_list1<true>(tv, nb, nullptr, L.l1_ptr, L.l1_src, s);
   if (!do_pw) return;
-  int lo = t.lev_start[t.ncutoff], n = t.lev_start[t.ncutoff + 1] - lo;
-  DBuf<int> ff(n, s), fe(n, s), pf(n, s), pe(n, s), tf(1, s), te(1, s), fslot(n, s);
-  k_pw_flags<<<grid_for(n, 128), 128, 0, s>>>(tv, t.ndiv, ff, fe);
-  FGT_LAUNCH_CHECK();
-  exclusive_scan_i32(ff, pf, n, tf, s);
-  exclusive_scan_i32(fe, pe, n, te, s);
-  L.n_form = fetch_int(tf, s);
-  L.n_eval = fetch_int(te, s);
   L.form_box.alloc(std::max(L.n_form, 1), s);
   L.eval_box.alloc(std::max(L.n_eval, 1), s);
   L.eval_self.alloc(std::max(L.n_eval, 1), s);

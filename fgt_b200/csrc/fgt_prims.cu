@@ -384,6 +384,25 @@ int fetch_int(const int* d, cudaStream_t s) {
   return h;
 }
 
+void fetch_ints(const int* const* d, int n, int* h, cudaStream_t s) {
+  // a per-thread pinned landing area: the copies queue behind each other
+  // and one synchronisation covers them all
+  struct Pinned {
+    int* p = nullptr;
+    ~Pinned() {
+      if (p) cudaFreeHost(p);
+    }
+  };
+  static thread_local Pinned buf;
+  constexpr int kMax = 16;
+  FGT_REQUIRE(n <= kMax, FGT_ERR_UNSUPPORTED, "too many values in one read-back");
+  if (!buf.p) FGT_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&buf.p), sizeof(int) * kMax, 0));
+  for (int i = 0; i < n; i++)
+    FGT_CUDA(cudaMemcpyAsync(buf.p + i, d[i], sizeof(int), cudaMemcpyDeviceToHost, s));
+  FGT_CUDA(cudaStreamSynchronize(s));
+  for (int i = 0; i < n; i++) h[i] = buf.p[i];
+}
+
 int unique_sorted_u64(const uint64_t* in, int n, uint64_t* out, cudaStream_t s) {
   if (n <= 0) return 0;
   DBuf<int> f(n, s), tot(1, s);

@@ -113,6 +113,8 @@ int unique_sorted_u64(const uint64_t* in, int n, uint64_t* out, cudaStream_t s);
 
 // Copy a device int to the host (synchronises the stream).
 int fetch_int(const int* d, cudaStream_t s);
+// Reads n (<= 16) device ints with one stream synchronisation.
+void fetch_ints(const int* const* d, int n, int* h, cudaStream_t s);
 
 __device__ __forceinline__ int dev_lower_bound(const uint64_t* a, int n, uint64_t v) {
   int lo = 0, hi = n;
