@@ -51,14 +51,17 @@ __host__ __device__ constexpr int fch() {
   return sizeof(T) == 4 ? 8192 : 2048;
 }
 
+constexpr int RD = 10;  // FP64 kernel row: one tile row (TILE <= RD - 1) + a zero
+
 // byte offset of the grid buffer in the tiled form kernel; every part is a
 // multiple of 16 bytes, so the kernel-row buffer is float4 aligned.  The
-// FP64 variant takes its kernel rows from warp shuffles (no row buffer).
+// FP64 variant's row buffer holds three rows of RD doubles per warp.
 template <typename T>
 __host__ __device__ constexpr size_t tiled_offset(int G, int K) {
   return tw_bytes16<T>(G, K) + sizeof(int) * (2 * NBLK_MAX + 32) + sizeof(int) * fch<T>() +
          sizeof(unsigned short) * fch<T>() +
-         (sizeof(T) == 4 ? sizeof(float) * (PW_THREADS / 32) * PB * 3 * TP : 0);
+         (sizeof(T) == 4 ? sizeof(float) * (PW_THREADS / 32) * PB * 3 * TP
+                         : sizeof(double) * (PW_THREADS / 32) * 3 * RD);
 }
 
 // Exclusive scan of cnt[0..n) into off[0..n) for n <= 2 * blockDim.x;
@@ -217,19 +220,22 @@ __device__ void spread_tiled(const PWArgs<T>& a, T* B, const double* __restrict_
 }
 
 // FP64 block-tiled spreading (3D, eps >= ~1e-6): as spread_tiled, with
-// blocks of TBD^3 base cells, a register tile of (TBD+W-1)^3 FP64 cells
-// (lane l owns the tile columns l, l+32, ... with all TILE z cells), and the
-// point's three kernel rows taken from warp shuffles: lanes 0..3W-1 each
-// evaluate one kernel value (dimension lane/W, offset lane%W) per point.  The
-// flush adds every non-zero tile cell with one atomic: ~TILE^3/(points per
-// block) atomics per point instead of W^3.
+// blocks of TBD^3 base cells and a register tile of (TBD+W-1)^3 FP64 cells
+// (lane l owns the tile columns l, l+32, ... with all TILE z cells).  Per
+// point, lane t < 3 RD writes entry t % RD of the point's kernel row t / RD
+// in tile coordinates (zero outside the stencil, the x row times the
+// strength) to the warp's row buffer, and every lane reads its values as
+// broadcasts: no shuffles and no edge selects.  The flush adds every
+// non-zero tile cell with one atomic: ~TILE^3/(points per block) atomics
+// per point instead of W^3.
 template <int W, int TBD>
 __device__ void spread_tiled_d(const PWArgs<double>& a, double* B, const double* __restrict__ off,
                                int ns, const double* __restrict__ sq,
                                const double* __restrict__ sr, bool is_q, int c0, int n, int* cnt,
-                               int* boff, int* misc, int* tmp, unsigned short* perm) {
+                               int* boff, int* misc, int* tmp, unsigned short* perm,
+                               double* rows) {
   constexpr int TILE = TBD + W - 1, NCOL = (TILE * TILE + 31) / 32;
-  static_assert(3 * W <= 32, "one kernel value per lane");
+  static_assert(TILE <= RD - 1 && 3 * RD <= 32, "one row entry per lane, a zero at RD - 1");
   const Geo& g = a.g;
   const int nbd = (g.G - W + 1 + TBD - 1) / TBD, nblk = nbd * nbd * nbd;
   for (int i = threadIdx.x; i < nblk; i += blockDim.x) cnt[i] = 0;
@@ -251,14 +257,16 @@ __device__ void spread_tiled_d(const PWArgs<double>& a, double* B, const double*
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
+  double* R = rows + (threadIdx.x >> 5) * 3 * RD;
+  // slots past the tile read entry RD - 1 of the rows, which stays zero
   int cx[NCOL], cy[NCOL];
 #pragma unroll
   for (int j = 0; j < NCOL; j++) {
     const int c = lane + 32 * j;
-    cx[j] = c < TILE * TILE ? c / TILE : -1;
-    cy[j] = c < TILE * TILE ? c % TILE : -1;
+    cx[j] = c < TILE * TILE ? c / TILE : RD - 1;
+    cy[j] = c < TILE * TILE ? c % TILE : RD - 1;
   }
-  const int kd = lane / W, kj = lane - kd * W;  // this lane's kernel value
+  const int kd = lane / RD, kq = lane - kd * RD;  // this lane's row entry
   for (;;) {
     int bi = 0;
     if (lane == 0) bi = atomicAdd(&misc[0], 1);
@@ -278,42 +286,38 @@ __device__ void spread_tiled_d(const PWArgs<double>& a, double* B, const double*
       for (int t = 0; t < TILE; t++) acc[j][t] = 0.0;
     for (int k = 0; k < nb; k++) {
       const int pt = c0 + perm[start + k];
-      // stencil offsets in the tile (all lanes) and this lane's kernel value
-      int o[3];
+      // this lane's row entry: kernel value at stencil offset kq - o[kd] of
+      // dimension kd (zero outside the stencil; the x row carries the strength)
       double v = 0.0;
-#pragma unroll
-      for (int d = 0; d < 3; d++) {
-        const double x = off[(size_t)d * ns + pt] * a.scale_d;
+      if (lane < 3 * RD) {
+        const double x = off[(size_t)kd * ns + pt] * a.scale_d;
         double f0;
-        const int i0 = kernel_start<double>(a, x, f0);
-        int b = i0 - g.l0;
+        int b = kernel_start<double>(a, x, f0) - g.l0;
         b = b < 0 ? 0 : (b > g.G - W ? g.G - W : b);
-        o[d] = b - org[d];
-        if (d == kd && lane < 3 * W) v = es_kernel<double>((f0 + (double)kj) * a.inv_hw, a.beta);
+        int j = kq - (b - (kd == 0 ? org[0] : (kd == 1 ? org[1] : org[2])));
+        if (!FGT_DCHECK(kq != RD - 1 || j >= W, 208)) j = W;  // entry RD - 1 stays zero
+        if (j >= 0 && j < W) {
+          v = es_kernel<double>((f0 + (double)j) * a.inv_hw, a.beta);
+          if (kd == 0) v *= is_q ? sq[pt] : sq[pt] * sr[pt];
+        }
+        R[lane] = v;
       }
-      const double sc = is_q ? sq[pt] : sq[pt] * sr[pt];
+      __syncwarp();
       double pz[TILE];
 #pragma unroll
-      for (int t = 0; t < TILE; t++) {
-        const int jz = t - o[2];
-        const double z = __shfl_sync(0xffffffffu, v, 2 * W + (jz < 0 ? 0 : (jz >= W ? W - 1 : jz)));
-        pz[t] = (jz >= 0 && jz < W) ? z : 0.0;
-      }
+      for (int t = 0; t < TILE; t++) pz[t] = R[2 * RD + t];
 #pragma unroll
       for (int j = 0; j < NCOL; j++) {
-        const int jx = cx[j] - o[0], jy = cy[j] - o[1];
-        const double px = __shfl_sync(0xffffffffu, v, jx < 0 ? 0 : (jx >= W ? W - 1 : jx));
-        const double py = __shfl_sync(0xffffffffu, v, W + (jy < 0 ? 0 : (jy >= W ? W - 1 : jy)));
-        const bool in = jx >= 0 && jx < W && jy >= 0 && jy < W;
-        const double pxy = in ? px * py * sc : 0.0;
+        const double pxy = R[cx[j]] * R[RD + cy[j]];
 #pragma unroll
         for (int t = 0; t < TILE; t++) acc[j][t] = fma(pxy, pz[t], acc[j][t]);
       }
+      __syncwarp();
     }
 #pragma unroll
     for (int j = 0; j < NCOL; j++) {
       const int x = org[0] + cx[j], y = org[1] + cy[j];
-      if (cx[j] >= 0 && x < g.G && y < g.G) {
+      if (lane + 32 * j < TILE * TILE && x < g.G && y < g.G) {
         double* col = B + x * g.str[0] + y * g.str[1] + org[2];
 #pragma unroll
         for (int t = 0; t < TILE; t++)
@@ -383,7 +387,7 @@ __global__ void __launch_bounds__(PW_THREADS) k_form(PWArgs<T> a, FormIO io, For
           for (int c0 = p0; c0 < p1; c0 += fch<T>()) {
             if constexpr (std::is_same<T, double>::value)
               spread_tiled_d<W, TB_D>(a, B, p.off, io.ns, sq, sr, is_q, c0, min(fch<T>(), p1 - c0),
-                                      tcnt, toff, tmisc, ttmp, tperm);
+                                      tcnt, toff, tmisc, ttmp, tperm, trows);
             else
               spread_tiled<T, W>(a, B, p.off, io.ns, sq, sr, is_q, c0, min(fch<T>(), p1 - c0),
                                  tcnt, toff, tmisc, ttmp, tperm, trows);
