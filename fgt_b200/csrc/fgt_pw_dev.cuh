@@ -716,6 +716,54 @@ __device__ __forceinline__ void interp_grad_point_s3(const PWArgs<float>& a, uin
   v[3] = gz;
 }
 
+// interp_grad_point for 3D grids without wrap-around, with the x weights
+// computed as the rolled x loop reaches them: only the y and z rows (values
+// and derivatives) stay in registers, so the FP64 stencil fits the 128
+// registers of a 512-thread CTA.  Same sums as interp_grad_cells.
+template <typename T, int W, class GV>
+__device__ __forceinline__ void interp_grad_point_xr(const PWArgs<T>& a, const GV& B,
+                                                     const double* x, T* v) {
+  T ph[2][W], dph[2][W];  // y and z rows
+  T f0x;
+  int s[3];
+  s[0] = kernel_start<T>(a, x[0], f0x);
+  s[1] = kernel_row_d<T, W>(a, x[1], ph[0], dph[0]);
+  s[2] = kernel_row_d<T, W>(a, x[2], ph[1], dph[1]);
+  const LinIdx<3, W> ix(a.g, s);
+  const T bref = B[ix.x(W / 2) + ix.y(W / 2) + ix.z(W / 2)];
+  T ksy = T(0), ksz = T(0), ksx = T(0);
+#pragma unroll
+  for (int j = 0; j < W; j++) {
+    ksy += ph[0][j];
+    ksz += ph[1][j];
+  }
+  T pot = T(0), gx = T(0), gy = T(0), gz = T(0);
+#pragma unroll 1
+  for (int jx = 0; jx < W; jx++) {
+    T px, dpx;
+    kernel_val_d<T>(a, f0x, jx, px, dpx);
+    ksx += px;
+    const auto bx = B + ix.x(jx);
+    T t0 = T(0), t1 = T(0), t2 = T(0);
+#pragma unroll
+    for (int jy = 0; jy < W; jy++) {
+      T s0, s1;
+      line_sums<T, W>(bx + ix.y(jy), ix, bref, ph[1], dph[1], s0, s1);
+      t0 += ph[0][jy] * s0;
+      t1 += dph[0][jy] * s0;
+      t2 += ph[0][jy] * s1;
+    }
+    pot += px * t0;
+    gx += dpx * t0;
+    gy += px * t1;
+    gz += px * t2;
+  }
+  v[0] = pot + bref * ((ksx * ksy) * ksz);
+  v[1] = gx;
+  v[2] = gy;
+  v[3] = gz;
+}
+
 template <typename T, int DIM, int W, class GV>
 __device__ __forceinline__ void interp_grad_point(const PWArgs<T>& a, const GV& B, const double* x,
                                                   T* v) {

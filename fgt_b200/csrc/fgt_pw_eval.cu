@@ -130,8 +130,11 @@ __device__ __forceinline__ void build_eval_grid(const PWArgs<T>& a, const T* L, 
 #endif
 template <typename T, int DIM, int W, bool GB, bool DERIV>
 constexpr int eval_threads() {
-  return (std::is_same<T, float>::value && DIM == 3 && W <= 9 && !GB && DERIV) ? FGT_EVAL3_THREADS
-                                                                               : PW_THREADS;
+  if constexpr (std::is_same<T, float>::value && DIM == 3 && W <= 9 && !GB && DERIV)
+    return FGT_EVAL3_THREADS;
+  // the FP64 derivative stencil needs more than 128 registers per thread
+  if constexpr (std::is_same<T, double>::value && DIM == 3 && DERIV) return PW_THREADS / 2;
+  return PW_THREADS;
 }
 
 template <typename T, int DIM, int W, bool GB, bool DERIV>
@@ -222,6 +225,11 @@ __global__ void __launch_bounds__(eval_threads<T, DIM, W, GB, DERIV>())
                 if constexpr (!GB && DIM == 3 && std::is_same<T, float>::value) {
                   if (!g.wrap)
                     interp_grad_point_s3<W>(a, grid_saddr, x, v);
+                  else
+                    interp_grad_point<T, DIM, W>(a, BV, x, v);
+                } else if constexpr (DIM == 3 && std::is_same<T, double>::value) {
+                  if (!g.wrap)
+                    interp_grad_point_xr<T, W>(a, BV, x, v);
                   else
                     interp_grad_point<T, DIM, W>(a, BV, x, v);
                 } else {
