@@ -297,6 +297,100 @@ __global__ void __launch_bounds__(RS_THREADS)
   }
 }
 
+// k_radix_scatter for 32-bit keys with the tile reordered in shared memory
+// first: the tile's items are ranked stably by digit (the same rank as
+// k_radix_scatter's), placed in digit order in shared memory, and then
+// written out by consecutive threads, so each digit's run of the tile goes
+// to consecutive global positions (whole sectors) instead of one scattered
+// 4-byte store per item.  Same output as k_radix_scatter.
+__global__ void __launch_bounds__(RS_THREADS)
+    k_radix_scatter_tile(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                         uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, int n,
+                         int shift, const int* __restrict__ offs, int nblocks) {
+  __shared__ uint32_t sk[RS_TILE];
+  __shared__ uint32_t sv[RS_TILE];
+  __shared__ int run[256];    // running count per digit, then the tile's digit start
+  __shared__ int gbase[256];  // global start of the tile's run of each digit
+  __shared__ int wc[RS_WARPS][256];
+  __shared__ int wsum[RS_WARPS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int tbase = blockIdx.x * RS_TILE;
+  const int tn = min(RS_TILE, n - tbase);
+  run[tid] = 0;
+  gbase[tid] = offs[tid * nblocks + blockIdx.x];
+  uint32_t key[RS_ITEMS], val[RS_ITEMS];
+  int rk[RS_ITEMS];
+#pragma unroll
+  for (int r = 0; r < RS_ITEMS; r++) {
+    const int i = tbase + r * RS_THREADS + tid;
+    const bool valid = i < n;
+    key[r] = valid ? kin[i] : 0u;
+    val[r] = (valid && vin) ? vin[i] : 0u;
+  }
+  __syncthreads();
+  // stable rank of every item among the tile's items of its digit
+#pragma unroll
+  for (int r = 0; r < RS_ITEMS; r++) {
+    const bool valid = tbase + r * RS_THREADS + tid < n;
+    const int d = valid ? (int)((key[r] >> shift) & 255u) : 256;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const bool leader = (__ffs(peers) - 1) == lane;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; w++) wc[w][tid] = 0;
+    __syncthreads();
+    if (valid && leader) wc[warp][d] = __popc(peers);
+    __syncthreads();
+    {
+      int c0 = run[tid];
+#pragma unroll
+      for (int w = 0; w < RS_WARPS; w++) {
+        const int c = wc[w][tid];
+        wc[w][tid] = c0;
+        c0 += c;
+      }
+      run[tid] = c0;
+    }
+    __syncthreads();
+    rk[r] = valid ? wc[warp][d] + __popc(peers & lt) : 0;
+    __syncthreads();
+  }
+  // exclusive scan of the tile's digit counts: digit starts in the tile
+  {
+    const int c = run[tid];
+    int inc = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += u;
+    }
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    int wo = 0;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; w++) wo += w < warp ? wsum[w] : 0;
+    run[tid] = wo + inc - c;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < RS_ITEMS; r++) {
+    if (tbase + r * RS_THREADS + tid < n) {
+      const int d = (int)((key[r] >> shift) & 255u);
+      const int slot = run[d] + rk[r];
+      sk[slot] = key[r];
+      sv[slot] = val[r];
+    }
+  }
+  __syncthreads();
+  for (int j = tid; j < tn; j += RS_THREADS) {
+    const uint32_t k = sk[j];
+    const int d = (int)((k >> shift) & 255u);
+    const int pos = gbase[d] + (j - run[d]);
+    kout[pos] = k;
+    if (vout) vout[pos] = sv[j];
+  }
+}
+
 __global__ void k_lower_bound(const uint64_t* __restrict__ a, int n, const uint64_t* __restrict__ q,
                               int m, int* __restrict__ out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
@@ -348,7 +442,10 @@ void radix_sort_t(K* keys, uint32_t* vals, K* ktmp, uint32_t* vtmp, int n, int b
     k_radix_hist<K><<<nb, RS_THREADS, 0, s>>>(ka, n, shift, hist, nb);
     FGT_LAUNCH_CHECK();
     exclusive_scan_i32(hist, hist, 256 * nb, nullptr, s);
-    k_radix_scatter<K><<<nb, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, shift, hist, nb);
+    if constexpr (sizeof(K) == 4)
+      k_radix_scatter_tile<<<nb, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, shift, hist, nb);
+    else
+      k_radix_scatter<K><<<nb, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, shift, hist, nb);
     FGT_LAUNCH_CHECK();
     std::swap(ka, kb);
     std::swap(va, vb);
