@@ -643,8 +643,10 @@ __global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal(PWArgs<T> a, EvalP
 // streamed through shared memory in chunks of whole rows (register
 // prefetch of the next chunk while the current one is summed), stored as
 // (w lr, w lr, -w li, w li) so that one 128-bit broadcast load and two packed
-// FP32x2 FMAs against the point's (er, ei, ei, er) give the complex product
-// of a mode.  Rows, lanes and the FP64 reduction as in k_eval_modal.
+// FP32x2 FMAs against the point's (er, ei) and (ei, er) give the complex
+// product of a mode; the point's factors are one 8-byte load per mode (the
+// shared-memory traffic of the loop is mostly these per-lane loads).  Rows,
+// lanes and the FP64 reduction as in k_eval_modal.
 constexpr int MODAL_CHUNK = 1024;  // modes per staged chunk (whole rows)
 template <int DIM>
 __host__ __device__ constexpr int modal32_ncg() { return 1 + DIM; }
@@ -668,8 +670,9 @@ __global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal32(PWArgs<float> a,
   const int nch = (nrows + rpc - 1) / rpc;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* red = reinterpret_cast<double*>(smem_raw);                 // [NW][32][NCG]
-  float4* Ez = reinterpret_cast<float4*>(red + (size_t)NW * 32 * NCG);  // [NH][pmax]
-  float4* Lb = Ez + (size_t)NH * pmax;                                // [2][MODAL_CHUNK]
+  // [NH][pmax] (cos, sin) of the last dimension (in a region sized for float4)
+  float2* Ez = reinterpret_cast<float2*>(red + (size_t)NW * 32 * NCG);
+  float4* Lb = reinterpret_cast<float4*>(Ez) + (size_t)NH * pmax;     // [2][MODAL_CHUNK]
   float2* Exy = reinterpret_cast<float2*>(Lb + 2 * MODAL_CHUNK);      // [(DIM-1) NF][pmax]
   float2* T2 = Exy + (size_t)(DIM - 1) * NF * pmax;                   // [NH] (t, t)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -694,7 +697,7 @@ __global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal32(PWArgs<float> a,
       double sn, cs;
       sincos(x * (double)k, &sn, &cs);
       const float c = (float)cs, sv = (float)sn;
-      if (d == DIM - 1) Ez[(size_t)k * pmax + pi] = make_float4(c, sv, sv, c);
+      if (d == DIM - 1) Ez[(size_t)k * pmax + pi] = make_float2(c, sv);
       else Exy[(size_t)r * pmax + pi] = make_float2(c, sv);
     }
     for (int id = 0; id < p.nd; id++) {
@@ -739,14 +742,14 @@ __global__ void __launch_bounds__(MODAL_THREADS) k_eval_modal32(PWArgs<float> a,
           if (act) {
             for (int r = r0 + ((rs - r0) % S + S) % S; r < r1; r += S) {
               const float4* Lr = Lc + (size_t)(r - r0) * NH;
-              const float4* Ep = Ez + pi;
+              const float2* Ep = Ez + pi;
               float2 s0 = make_float2(0.f, 0.f), s1 = make_float2(0.f, 0.f);
 #pragma unroll 4
               for (int kz = 0; kz < NH; kz++) {
                 const float4 L4 = Lr[kz];
-                const float4 e4 = Ep[(size_t)kz * pmax];
-                float2 pr = __fmul2_rn(make_float2(L4.x, L4.y), make_float2(e4.x, e4.y));
-                pr = __ffma2_rn(make_float2(L4.z, L4.w), make_float2(e4.z, e4.w), pr);
+                const float2 e2 = Ep[(size_t)kz * pmax];
+                float2 pr = __fmul2_rn(make_float2(L4.x, L4.y), e2);
+                pr = __ffma2_rn(make_float2(L4.z, L4.w), make_float2(e2.y, e2.x), pr);
                 s0 = __fadd2_rn(s0, pr);
                 if (GRAD) s1 = __ffma2_rn(T2[kz], pr, s1);
               }
