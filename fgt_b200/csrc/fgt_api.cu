@@ -4,6 +4,7 @@
 // set-up (cut-off level, root box, expansion length, PW nodes) with the
 // reference's formulas.
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -11,6 +12,8 @@
 #include <mutex>
 #include <string>
 #include <vector>
+
+#include <nvtx3/nvToolsExt.h>  // header-only NVTX v3: no library to link
 
 #include "fgt_pw.cuh"
 
@@ -274,6 +277,13 @@ struct SideSync {
   }
 };
 
+// Phase names of fgt_stats.ms (slots 0..9).
+const char* const kPhaseName[10] = {"h2d",       "tree",  "sort_gather", "lists", "form",
+                                    "translate", "eval",  "direct",      "scatter", "d2h"};
+
+// Phase boundaries of a call: CUDA events on the call's stream when timing
+// is on, and always an NVTX marker "fgt <phase> done" for profilers
+// (nothing happens unless a tool is attached).  mark(k) ends phase k.
 struct Timer {
   bool on;
   cudaStream_t s;
@@ -281,6 +291,11 @@ struct Timer {
   std::vector<int> slot;
   Timer(bool o, cudaStream_t st) : on(o), s(st) {}
   void mark(int phase_slot) {
+    if (phase_slot >= 0 && phase_slot < 10) {
+      char name[48];
+      snprintf(name, sizeof(name), "fgt %s done", kPhaseName[phase_slot]);
+      nvtxMarkA(name);
+    }
     if (!on) return;
     cudaEvent_t e;
     FGT_CUDA(cudaEventCreate(&e));
@@ -763,6 +778,40 @@ bool fault_requested(const char* what) {
   return f && strstr(f, what) != nullptr;
 }
 
+// FGT_LOG=1 (any value but "0"): every pfgt call times its phases and
+// writes one JSON line to stderr with the tree and list sizes, the per-phase
+// device times and the achieved rates of the form, evaluation, near-field
+// and translation kernels.  Silent by default.
+bool log_requested() {
+  const char* f = getenv("FGT_LOG");
+  return f && *f && strcmp(f, "0") != 0;
+}
+
+void log_call(const fgt_stats& st, int nd, int dim, int ns, int nt, double delta, double eps) {
+  static std::mutex mu;
+  char ms[512];
+  int k = snprintf(ms, sizeof(ms), "{");
+  for (int i = 0; i < 10; i++)
+    k += snprintf(ms + k, sizeof(ms) - k, "%s\"%s\": %.4f", i ? ", " : "", kPhaseName[i],
+                  st.ms[i]);
+  snprintf(ms + k, sizeof(ms) - k, ", \"total\": %.4f}", st.ms[10]);
+  auto rate = [](double work, double msec) { return msec > 0 ? work / (msec * 1e-3) : 0.0; };
+  std::lock_guard<std::mutex> lk(mu);
+  fprintf(stderr,
+          "{\"fgt\": \"pfgt\", \"nd\": %d, \"dim\": %d, \"ns\": %d, \"nt\": %d, "
+          "\"delta\": %.6g, \"eps\": %.6g, \"precision\": \"%s\", \"nlevels\": %d, "
+          "\"nboxes\": %d, \"npwlevel\": %d, \"npw\": %d, \"n_form_boxes\": %d, "
+          "\"n_eval_boxes\": %d, \"n_translations\": %d, \"near_pairs\": %.6g, "
+          "\"kernel_launches\": %d, \"ms\": %s, \"tflops\": {\"form\": %.4g, "
+          "\"eval\": %.4g, \"direct\": %.4g}, \"translate_gbs\": %.4g}\n",
+          nd, dim, ns, nt, delta, eps, st.precision_used == FGT_PREC_FP64 ? "fp64" : "mixed",
+          st.nlevels, st.nboxes, st.npwlevel, st.npw, st.n_form_boxes, st.n_eval_boxes,
+          st.n_translations, st.near_pairs, st.n_kernel_launches, ms,
+          rate(st.flops_form, st.ms[4]) * 1e-12, rate(st.flops_eval, st.ms[6]) * 1e-12,
+          rate(st.flops_direct, st.ms[7]) * 1e-12, rate(st.bytes_translate, st.ms[5]) * 1e-9);
+  fflush(stderr);
+}
+
 // Device-side failures of a call, read after its last synchronisation:
 // a bounded wait that ran out (FGT_ERR_TIMEOUT) and, in the FGT_CHECK build,
 // a failed bounds check (FGT_ERR_CHECK, the first failing site named).
@@ -830,9 +879,10 @@ int pfgt_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps
   cudaStream_t s = o.stream ? (cudaStream_t)o.stream : library_stream(dev);
   ArenaScope arena_scope(s);
   fgt_stats local_stats;
-  fgt_stats* st = o.stats ? o.stats : nullptr;
+  const bool logging = log_requested();
+  fgt_stats* st = o.stats ? o.stats : (logging ? &local_stats : nullptr);
   if (st) memset(st, 0, sizeof(*st));
-  Timer tm(o.timing && st, s);
+  Timer tm((o.timing || logging) && st, s);
   int nhess = dim * (dim + 1) / 2;
   int prec = o.precision;
   if (prec == FGT_PREC_AUTO) prec = (eps >= 1e-6 * (1 - 1e-9)) ? FGT_PREC_MIXED : FGT_PREC_FP64;
@@ -917,8 +967,8 @@ int pfgt_impl(const fgt_opts* opts_in, int nd, int dim, double delta, double eps
   if (st) {
     st->precision_used = prec;
     tm.finish(st->ms);
+    if (logging) log_call(*st, nd, dim, ns, nt, delta, eps);
   }
-  (void)local_stats;
   return FGT_OK;
 }
 

@@ -1,5 +1,5 @@
 // Device helpers shared by the plane-wave form/translate kernels (K6, K7,
-// fgt_pw.cu) and the evaluation kernels (K8, fgt_pw_eval.cu).
+// fgt_pw.cu) and the evaluation kernels (K8, fgt_pw_eval_impl.cuh).
 //
 // Per box, one CTA keeps the whole spreading sub-grid in shared memory (a
 // global-memory slice per CTA when it does not fit): spread (ES kernel,

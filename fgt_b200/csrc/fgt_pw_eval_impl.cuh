@@ -1,5 +1,8 @@
 // Plane-wave evaluation kernels (K8): per-box grids with interpolation at
 // the box's points, and direct modal sums for boxes with few points.
+// Included by fgt_pw_eval_f32.cu and fgt_pw_eval_f64.cu, which instantiate
+// pw_eval for one arithmetic type each (the two halves compile in parallel).
+#pragma once
 #include <math.h>
 
 #include <algorithm>
@@ -1241,12 +1244,5 @@ int pw_eval(const PWParams& P, const Tree& t, const Lists& L, const PWData<T>& D
   }
   return launches;
 }
-
-template int pw_eval<float>(const PWParams&, const Tree&, const Lists&, const PWData<float>&,
-                            const EvalSet<float>&, const EvalSet<float>&, int, PWWork*,
-                            cudaStream_t);
-template int pw_eval<double>(const PWParams&, const Tree&, const Lists&, const PWData<double>&,
-                             const EvalSet<double>&, const EvalSet<double>&, int, PWWork*,
-                             cudaStream_t);
 
 }  // namespace fgt
